@@ -1,0 +1,597 @@
+// ecg_abi.cu -- host side of libecgb200.so: context lifetime, the GHEPIIS
+// driver and the EnergyIA / EnergyIB glue behind the C ABI in ecg_abi.h.
+#include <float.h>
+#include <math.h>
+#include <string.h>
+#include <algorithm>
+#include <new>
+#include "../../include/ecg_abi.h"
+#include "ecg_internal.h"
+
+using namespace ecg;
+
+struct ecg_ctx {
+    Ctx c;
+};
+
+#define CK(call)                                  \
+    do {                                          \
+        if ((call) != cudaSuccess) {              \
+            cudaGetLastError();                   \
+            return ECG_ECUDA;                     \
+        }                                         \
+    } while (0)
+#define CKR(expr)                                 \
+    do {                                          \
+        const int _r = (expr);                    \
+        if (_r != 0) return _r == -3 ? ECG_ENOMEM : (_r == -1 ? ECG_EARG : ECG_ECUDA); \
+    } while (0)
+
+namespace {
+
+constexpr int SOLVE_G_MAX = 64;
+
+template <typename T>
+int dalloc(T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) return 0;
+    if (cudaMalloc((void**)p, count * sizeof(T)) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return ECG_ENOMEM;
+    }
+    return 0;
+}
+
+void free_ctx(Ctx& c)
+{
+    void* ptrs[] = {c.params, c.H, c.S, c.diagS, c.diagH, c.invD, c.c, c.x, c.w, c.D, c.grad, c.Pd, c.coef,
+                    c.bra, c.ket, c.detL, c.part, c.dw, c.linv, c.vbuf, c.status, c.red, c.counters, c.yv,
+                    c.zv, c.spart, c.colval};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (c.status_h) cudaFreeHost(c.status_h);
+    if (c.red_h) cudaFreeHost(c.red_h);
+    if (c.stream) {
+        for (int i = 0; i < 16; i++) cudaEventDestroy(c.ev[i]);
+        cudaStreamDestroy(c.stream);
+    }
+}
+
+void mark(Ctx& c, int i)
+{
+    if (c.timing) cudaEventRecord(c.ev[i], c.stream);
+}
+
+double elapsed(Ctx& c, int a, int b)
+{
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c.ev[a], c.ev[b]) != cudaSuccess) {
+        cudaGetLastError();
+        return 0.0;
+    }
+    return ms;
+}
+
+int read_red(Ctx& c)
+{
+    CK(cudaMemcpyAsync(c.red_h, c.red, RD_COUNT * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return 0;
+}
+
+int compute_hs(Ctx& c, int nmin, int nmax, double approx_e)
+{
+    if (nmin < 1 || nmax < nmin || nmax > c.ld) return ECG_EARG;
+    CKR(launch_prep(c, nmax));
+    CKR(launch_pair_diag(c, nmin - 1, nmax, approx_e, 0, 0));
+    CKR(launch_pair_energy(c, nmin - 1, nmax, approx_e));
+    return 0;
+}
+
+int compute_hsd(Ctx& c, int nmin, int nmax, int nfru, double approx_e)
+{
+    if (nmin < 1 || nmax < nmin || nmax > c.ld || nfru < 0 || nfru >= nmin) return ECG_EARG;
+    if (nmax - nfru > c.max_nfo) return ECG_EARG;
+    if (!c.D) {
+        const size_t cnt = (size_t)2 * c.npt * c.max_nfo * c.ld;
+        if (dalloc(&c.D, cnt)) return ECG_ENOMEM;
+    }
+    CKR(launch_prep(c, nmax));
+    CKR(launch_pair_diag(c, nmin - 1, nmax, approx_e, 1, nfru));
+    CKR(launch_pair_plain_grad(c, nmin - 1, nmax, nfru, approx_e));
+    return 0;
+}
+
+// GHEPIIS, src/linalg.f90:1781-1926.
+int ghepiis(Ctx& c, int k, int n, double apprlambda, double tol, int max_iter, int specif_norm, double* lambda,
+            double* rel_acc, int* num_iter)
+{
+    if (c.method != 'I') return ECG_EARG;
+    if (k < 1 || n < k || n > c.ld || max_iter < 0) return ECG_EARG;
+    *rel_acc = DBL_MAX;
+    *num_iter = 0;
+    CK(cudaMemsetAsync(c.status, 0, ST_COUNT * sizeof(int), c.stream));
+    CKR(ldlh_factor(c, k - 1, n));
+    CK(cudaMemcpyAsync(c.status_h, c.status, ST_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    mark(c, 2);
+    if (c.status_h[ST_ZERO_PIVOT] != 0) {
+        // LDLHF returned ErrorCode = 1 (src/linalg.f90:377-380); the factor
+        // is incomplete, so no row of it may be reused.
+        c.fact_n = 0;
+        c.blk_start.clear();
+        mark(c, 3);
+        return ECG_ESINGULAR;
+    }
+    bool notconverged = true;
+    double nd = 0.0, prev = DBL_MAX;
+    int it = 0;
+    while (notconverged && it < max_iter) {
+        CKR(invit_step(c, n, it == 0));
+        CKR(read_red(c));
+        nd = c.red_h[RD_NORMDIFF];
+        if (tol > 0.0) {
+            if (nd <= tol) notconverged = false;
+        } else {
+            if (nd > prev && nd <= fabs(tol)) notconverged = false;
+            prev = nd;
+        }
+        it++;
+    }
+    mark(c, 3);
+    *rel_acc = nd;
+    *num_iter = it;
+    c.last_numiter = it;
+    CKR(invit_rayleigh(c, n));
+    CKR(read_red(c));
+    const double t1 = c.red_h[RD_T1], t2 = c.red_h[RD_T2];
+    *lambda = t2 / t1 + apprlambda;
+    if (specif_norm == 0) {
+        CKR(vec_scale(c, c.x, n, 1.0 / sqrt(t1)));
+    } else if (specif_norm == 1) {
+        CKR(vec_scale(c, c.x, n, 1.0 / sqrt(c.red_h[RD_XX])));
+    }
+    return notconverged ? ECG_ENOCONV : ECG_OK;
+}
+
+int single_function_energy(Ctx& c, double approx_e, double* energy)
+{
+    cd h11;
+    CK(cudaMemcpyAsync(&h11, c.H, sizeof(cd), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    *energy = h11.x + approx_e;
+    const cd one{1.0, 0.0};
+    CK(cudaMemcpyAsync(c.c, &one, sizeof(cd), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return 0;
+}
+
+void finish_timing(Ctx& c, bool grad)
+{
+    if (!c.timing) return;
+    cudaStreamSynchronize(c.stream);
+    c.stage_ms[0] = elapsed(c, 0, 1);
+    c.stage_ms[1] = elapsed(c, 1, 2);
+    c.stage_ms[2] = elapsed(c, 2, 3);
+    c.stage_ms[3] = grad ? elapsed(c, 3, 4) : 0.0;
+}
+
+int energy_ib_common(Ctx& c, int nfru, int nfa, int needed, double approx_e, double tol, int max_iter,
+                     double* energy, double* grad_host, int* num_iter, bool adjoint)
+{
+    if (c.method != 'I') return ECG_EARG;
+    if (nfru < 0 || nfa <= nfru || nfa > c.ld) return ECG_EARG;
+    const int nfo = nfa - nfru;
+    mark(c, 0);
+    if (needed) {
+        const int r = adjoint ? compute_hs(c, nfru + 1, nfa, approx_e) : compute_hsd(c, nfru + 1, nfa, nfru, approx_e);
+        if (r) return r;
+    } else if (!adjoint && !c.D) {
+        return ECG_EARG;
+    }
+    mark(c, 1);
+    int err = 0;
+    if (nfa == 1) {
+        mark(c, 2);
+        const int r = single_function_energy(c, approx_e, energy);
+        if (r) return r;
+        *num_iter = 1;
+        mark(c, 3);
+    } else {
+        CK(cudaMemcpyAsync(c.c, c.x, (size_t)nfa * sizeof(cd), cudaMemcpyDeviceToDevice, c.stream));
+        double lam = 0.0, ra = 0.0;
+        int it = 0;
+        err = ghepiis(c, nfru + 1, nfa, approx_e, tol, max_iter, 0, &lam, &ra, &it);
+        if (err < 0) return err;
+        if (err == ECG_ESINGULAR) {
+            *num_iter = 0;
+            return err;
+        }
+        *energy = lam;
+        *num_iter = it;
+        // Glob_c(1:nfa) = Glob_LastEigvector(1:nfa), src/workproc.f90:2114
+        CK(cudaMemcpyAsync(c.c, c.x, (size_t)nfa * sizeof(cd), cudaMemcpyDeviceToDevice, c.stream));
+    }
+    if (adjoint) {
+        CKR(launch_adjoint(c, nfru, nfa, *energy));
+    } else {
+        CKR(launch_plain_contract(c, nfo, nfa, nfru, *energy));
+    }
+    mark(c, 4);
+    if (grad_host) {
+        CK(cudaMemcpyAsync(grad_host, c.grad, (size_t)nfo * c.npt * sizeof(double), cudaMemcpyDeviceToHost,
+                           c.stream));
+    }
+    CK(cudaStreamSynchronize(c.stream));
+    finish_timing(c, true);
+    return err;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_host, int nterms,
+                   const int* yhy_mats_host, const int* yhy_coeffs_host, int ld, int max_nfo, char method,
+                   int device, ecg_ctx** out)
+{
+    if (!out) return ECG_EARG;
+    *out = nullptr;
+    if (n < 2 || n > NMAX || nterms < 1 || nterms > TMAX || ld < 1 || max_nfo < 0 || max_nfo > ld) return ECG_EARG;
+    if (method != 'I' && method != 'G') return ECG_EARG;
+    if (!mass_matrix_host || !charges_host || !yhy_mats_host || !yhy_coeffs_host) return ECG_EARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return ECG_ENODEV;
+    }
+    if (device < 0 || device >= ndev) return ECG_EARG;
+    CK(cudaSetDevice(device));
+    ecg_ctx* h = new (std::nothrow) ecg_ctx();
+    if (!h) return ECG_ENOMEM;
+    Ctx& c = h->c;
+    c.dev = device;
+    c.n = n;
+    c.np = n * (n + 1) / 2;
+    c.npt = 2 * c.np;
+    c.T = nterms;
+    c.ld = ld;
+    c.max_nfo = max_nfo;
+    c.method = method;
+    memset(&c.sp, 0, sizeof(c.sp));
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) c.sp.M[i * NMAX + j] = mass_matrix_host[i + j * n];
+    c.sp.q0 = charges_host[0];
+    for (int i = 0; i < n; i++) c.sp.q[i] = charges_host[1 + i];
+    c.sp.two_r3n2 = pow(2.0, (3 * n) / 2.0);
+    c.sp.n = n;
+    c.sp.T = nterms;
+    std::vector<double> P((size_t)nterms * NMAX * NMAX, 0.0), cf(nterms);
+    for (int t = 0; t < nterms; t++) {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) P[((size_t)t * NMAX + i) * NMAX + j] = yhy_mats_host[(size_t)t * n * n + i + j * n];
+        cf[t] = yhy_coeffs_host[t];
+    }
+    int r = 0;
+    if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete h;
+        return ECG_ECUDA;
+    }
+    for (int i = 0; i < 16; i++) cudaEventCreate(&c.ev[i]);
+    const size_t L = (size_t)ld;
+    r |= dalloc(&c.params, (size_t)c.npt * L);
+    r |= dalloc(&c.H, L * L);
+    r |= dalloc(&c.S, L * L);
+    r |= dalloc(&c.diagS, L);
+    r |= dalloc(&c.diagH, L);
+    r |= dalloc(&c.invD, L);
+    r |= dalloc(&c.c, L);
+    r |= dalloc(&c.x, L);
+    r |= dalloc(&c.w, L);
+    r |= dalloc(&c.yv, L);
+    r |= dalloc(&c.zv, L);
+    r |= dalloc(&c.grad, (size_t)c.npt * L);
+    r |= dalloc(&c.Pd, P.size());
+    r |= dalloc(&c.coef, (size_t)nterms);
+    r |= dalloc(&c.bra, L * c.np);
+    r |= dalloc(&c.ket, L * nterms * c.np);
+    r |= dalloc(&c.detL, L);
+    r |= dalloc(&c.dw, L);
+    r |= dalloc(&c.linv, L * LDL_NB);
+    r |= dalloc(&c.vbuf, L * LDL_NB);
+    r |= dalloc(&c.status, (size_t)ST_COUNT);
+    r |= dalloc(&c.red, (size_t)RD_COUNT);
+    r |= dalloc(&c.counters, (size_t)4);
+    r |= dalloc(&c.spart, (size_t)SOLVE_G_MAX * LDL_NB);
+    r |= dalloc(&c.colval, 2 * L);
+    if (!r) {
+        if (cudaMallocHost((void**)&c.status_h, ST_COUNT * sizeof(int)) != cudaSuccess ||
+            cudaMallocHost((void**)&c.red_h, RD_COUNT * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            r = ECG_ENOMEM;
+        }
+    }
+    if (r) {
+        free_ctx(c);
+        delete h;
+        return ECG_ENOMEM;
+    }
+    bool ok = cudaMemcpy(c.Pd, P.data(), P.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(c.coef, cf.data(), cf.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemset(c.H, 0, L * L * sizeof(cd)) == cudaSuccess &&
+              cudaMemset(c.S, 0, L * L * sizeof(cd)) == cudaSuccess &&
+              cudaMemset(c.counters, 0, 4 * sizeof(int)) == cudaSuccess &&
+              cudaMemset(c.status, 0, ST_COUNT * sizeof(int)) == cudaSuccess &&
+              cudaMemset(c.c, 0, L * sizeof(cd)) == cudaSuccess && cudaMemset(c.x, 0, L * sizeof(cd)) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        free_ctx(c);
+        delete h;
+        return ECG_ECUDA;
+    }
+    *out = h;
+    return ECG_OK;
+}
+
+int ecg_ctx_destroy(ecg_ctx* ctx)
+{
+    if (!ctx) return ECG_EARG;
+    cudaSetDevice(ctx->c.dev);
+    cudaStreamSynchronize(ctx->c.stream);
+    free_ctx(ctx->c);
+    delete ctx;
+    return ECG_OK;
+}
+
+int ecg_set_params(ecg_ctx* ctx, const double* params_host, int first, int count)
+{
+    if (!ctx || !params_host || first < 1 || count < 0 || first - 1 + count > ctx->c.ld) return ECG_EARG;
+    Ctx& c = ctx->c;
+    CK(cudaMemcpyAsync(c.params + (size_t)(first - 1) * c.npt, params_host, (size_t)count * c.npt * sizeof(double),
+                       cudaMemcpyHostToDevice, c.stream));
+    return ECG_OK;
+}
+
+int ecg_compute_mat_elem(ecg_ctx* ctx, int nmin, int nmax, double approx_energy)
+{
+    if (!ctx) return ECG_EARG;
+    Ctx& c = ctx->c;
+    mark(c, 0);
+    const int r = compute_hs(c, nmin, nmax, approx_energy);
+    mark(c, 1);
+    if (r) return r;
+    if (c.timing) {
+        cudaStreamSynchronize(c.stream);
+        c.stage_ms[0] = elapsed(c, 0, 1);
+    }
+    return ECG_OK;
+}
+
+int ecg_compute_mat_elem_and_deriv(ecg_ctx* ctx, int nmin, int nmax, int nfru, double approx_energy)
+{
+    if (!ctx) return ECG_EARG;
+    Ctx& c = ctx->c;
+    mark(c, 0);
+    const int r = compute_hsd(c, nmin, nmax, nfru, approx_energy);
+    mark(c, 1);
+    if (r) return r;
+    if (c.timing) {
+        cudaStreamSynchronize(c.stream);
+        c.stage_ms[0] = elapsed(c, 0, 1);
+    }
+    return ECG_OK;
+}
+
+int ecg_ghepiis(ecg_ctx* ctx, int k, int n, double apprlambda, double tol, int max_iter, int specif_norm,
+                double* lambda, double* rel_acc, int* num_iter)
+{
+    if (!ctx || !lambda || !rel_acc || !num_iter) return ECG_EARG;
+    Ctx& c = ctx->c;
+    mark(c, 1);
+    const int r = ghepiis(c, k, n, apprlambda, tol, max_iter, specif_norm, lambda, rel_acc, num_iter);
+    cudaStreamSynchronize(c.stream);
+    if (c.timing) {
+        c.stage_ms[1] = elapsed(c, 1, 2);
+        c.stage_ms[2] = elapsed(c, 2, 3);
+    }
+    return r;
+}
+
+int ecg_energy_ia(ecg_ctx* ctx, int nmin, int nmax, int mat_elem_needed, double approx_energy, double tol,
+                  int max_iter, int specif_norm, double* energy, int* num_iter)
+{
+    if (!ctx || !energy || !num_iter) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (c.method != 'I') return ECG_EARG;
+    if (nmin < 1 || nmax < nmin || nmax > c.ld) return ECG_EARG;
+    mark(c, 0);
+    if (mat_elem_needed) {
+        const int r = compute_hs(c, nmin, nmax, approx_energy);
+        if (r) return r;
+    }
+    mark(c, 1);
+    if (nmax == 1) {
+        mark(c, 2);
+        const int r = single_function_energy(c, approx_energy, energy);
+        mark(c, 3);
+        *num_iter = 1;
+        finish_timing(c, false);
+        return r;
+    }
+    // Glob_c(1:Nmax) = Glob_LastEigvector(1:Nmax), src/workproc.f90:1989
+    CK(cudaMemcpyAsync(c.c, c.x, (size_t)nmax * sizeof(cd), cudaMemcpyDeviceToDevice, c.stream));
+    double lam = 0.0, ra = 0.0;
+    int it = 0;
+    const int r = ghepiis(c, nmin, nmax, approx_energy, tol, max_iter, specif_norm, &lam, &ra, &it);
+    *num_iter = it;
+    if (r >= 0 && r != ECG_ESINGULAR) *energy = lam;
+    finish_timing(c, false);
+    return r;
+}
+
+int ecg_energy_ib(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, double approx_energy, double tol,
+                  int max_iter, double* energy, double* grad_host, int* num_iter)
+{
+    if (!ctx || !energy || !num_iter) return ECG_EARG;
+    return energy_ib_common(ctx->c, nfru, nfa, mat_elem_needed, approx_energy, tol, max_iter, energy, grad_host,
+                            num_iter, false);
+}
+
+int ecg_energy_ib_adjoint(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, double approx_energy, double tol,
+                          int max_iter, double* energy, double* grad_host, int* num_iter)
+{
+    if (!ctx || !energy || !num_iter) return ECG_EARG;
+    return energy_ib_common(ctx->c, nfru, nfa, mat_elem_needed, approx_energy, tol, max_iter, energy, grad_host,
+                            num_iter, true);
+}
+
+int ecg_get_matrices(ecg_ctx* ctx, int n, double* H_host, double* S_host, int ld_host, double* diagS_host,
+                     double* diagH_host, double* invD_host)
+{
+    if (!ctx || n < 0 || n > ctx->c.ld) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if ((H_host || S_host) && ld_host < n) return ECG_EARG;
+    const size_t w = (size_t)n * sizeof(cd);
+    if (n > 0) {
+        if (H_host)
+            CK(cudaMemcpy2DAsync(H_host, (size_t)ld_host * sizeof(cd), c.H, (size_t)c.ld * sizeof(cd), w, n,
+                                 cudaMemcpyDeviceToHost, c.stream));
+        if (S_host)
+            CK(cudaMemcpy2DAsync(S_host, (size_t)ld_host * sizeof(cd), c.S, (size_t)c.ld * sizeof(cd), w, n,
+                                 cudaMemcpyDeviceToHost, c.stream));
+        if (diagS_host)
+            CK(cudaMemcpyAsync(diagS_host, c.diagS, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        if (diagH_host)
+            CK(cudaMemcpyAsync(diagH_host, c.diagH, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        if (invD_host) CK(cudaMemcpyAsync(invD_host, c.invD, w, cudaMemcpyDeviceToHost, c.stream));
+    }
+    CK(cudaStreamSynchronize(c.stream));
+    return ECG_OK;
+}
+
+int ecg_get_vectors(ecg_ctx* ctx, int n, double* c_host, double* last_eigvec_host)
+{
+    if (!ctx || n < 0 || n > ctx->c.ld) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (n > 0 && c_host) CK(cudaMemcpyAsync(c_host, c.c, n * sizeof(cd), cudaMemcpyDeviceToHost, c.stream));
+    if (n > 0 && last_eigvec_host)
+        CK(cudaMemcpyAsync(last_eigvec_host, c.x, n * sizeof(cd), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return ECG_OK;
+}
+
+int ecg_set_vectors(ecg_ctx* ctx, int n, const double* c_host, const double* last_eigvec_host)
+{
+    if (!ctx || n < 0 || n > ctx->c.ld) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (n > 0 && c_host) CK(cudaMemcpyAsync(c.c, c_host, n * sizeof(cd), cudaMemcpyHostToDevice, c.stream));
+    if (n > 0 && last_eigvec_host)
+        CK(cudaMemcpyAsync(c.x, last_eigvec_host, n * sizeof(cd), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return ECG_OK;
+}
+
+int ecg_get_gradient(ecg_ctx* ctx, int nfo, double* grad_host)
+{
+    if (!ctx || !grad_host || nfo < 0 || nfo > ctx->c.ld) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (nfo > 0)
+        CK(cudaMemcpyAsync(grad_host, c.grad, (size_t)nfo * c.npt * sizeof(double), cudaMemcpyDeviceToHost,
+                           c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return ECG_OK;
+}
+
+int ecg_get_deriv(ecg_ctx* ctx, int nfo, int nfa, double* D_host)
+{
+    if (!ctx || !D_host) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (!c.D || nfo < 1 || nfo > c.max_nfo || nfa < 1 || nfa > c.ld) return ECG_EARG;
+    const size_t n2 = (size_t)2 * c.npt;
+    CK(cudaMemcpy2DAsync(D_host, n2 * nfo * sizeof(cd), c.D, n2 * c.max_nfo * sizeof(cd), n2 * nfo * sizeof(cd), nfa,
+                         cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return ECG_OK;
+}
+
+int ecg_matrix_elements(ecg_ctx* ctx, int count, const double* pk_host, const double* pl_host,
+                        const int* term_host, int gradflag, double* hs_host, double* dk_host, double* dl_host)
+{
+    if (!ctx || count < 0 || !pk_host || !pl_host || !term_host || !hs_host) return ECG_EARG;
+    Ctx& c = ctx->c;
+    for (int i = 0; i < count; i++)
+        if (term_host[i] < 0 || term_host[i] >= c.T) return ECG_EARG;
+    if (((gradflag == 1 || gradflag == 3) && !dk_host) || ((gradflag == 2 || gradflag == 3) && !dl_host))
+        return ECG_EARG;
+    if (count == 0) return ECG_OK;
+    const size_t npt = c.npt, nd = (size_t)4 * c.np;
+    double *pk = nullptr, *pl = nullptr;
+    int* term = nullptr;
+    cd *hs = nullptr, *dk = nullptr, *dl = nullptr;
+    int r = 0;
+    r |= dalloc(&pk, npt * count);
+    r |= dalloc(&pl, npt * count);
+    r |= dalloc(&term, (size_t)count);
+    r |= dalloc(&hs, (size_t)2 * count);
+    r |= dalloc(&dk, nd * count);
+    r |= dalloc(&dl, nd * count);
+    int status = r ? ECG_ENOMEM : ECG_OK;
+    if (!status) {
+        bool ok = cudaMemcpyAsync(pk, pk_host, npt * count * sizeof(double), cudaMemcpyHostToDevice, c.stream) ==
+                      cudaSuccess &&
+                  cudaMemcpyAsync(pl, pl_host, npt * count * sizeof(double), cudaMemcpyHostToDevice, c.stream) ==
+                      cudaSuccess &&
+                  cudaMemcpyAsync(term, term_host, count * sizeof(int), cudaMemcpyHostToDevice, c.stream) ==
+                      cudaSuccess;
+        if (ok && launch_term_batch(c, count, pk, pl, term, gradflag, hs, dk, dl) == 0) {
+            ok = cudaMemcpyAsync(hs_host, hs, 2 * count * sizeof(cd), cudaMemcpyDeviceToHost, c.stream) ==
+                 cudaSuccess;
+            if (ok && (gradflag == 1 || gradflag == 3))
+                ok = cudaMemcpyAsync(dk_host, dk, nd * count * sizeof(cd), cudaMemcpyDeviceToHost, c.stream) ==
+                     cudaSuccess;
+            if (ok && (gradflag == 2 || gradflag == 3))
+                ok = cudaMemcpyAsync(dl_host, dl, nd * count * sizeof(cd), cudaMemcpyDeviceToHost, c.stream) ==
+                     cudaSuccess;
+            ok = ok && cudaStreamSynchronize(c.stream) == cudaSuccess;
+        } else {
+            ok = false;
+        }
+        if (!ok) {
+            cudaGetLastError();
+            status = ECG_ECUDA;
+        }
+    }
+    cudaStreamSynchronize(c.stream);
+    void* ptrs[] = {pk, pl, term, hs, dk, dl};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    return status;
+}
+
+long long ecg_launch_count(ecg_ctx* ctx) { return ctx ? ctx->c.launches : -1; }
+
+int ecg_set_timing(ecg_ctx* ctx, int on)
+{
+    if (!ctx) return ECG_EARG;
+    ctx->c.timing = (on != 0);
+    return ECG_OK;
+}
+
+int ecg_get_stage_ms(ecg_ctx* ctx, double* ms4)
+{
+    if (!ctx || !ms4) return ECG_EARG;
+    for (int i = 0; i < 4; i++) ms4[i] = ctx->c.stage_ms[i];
+    return ECG_OK;
+}
+
+int ecg_sync(ecg_ctx* ctx)
+{
+    if (!ctx) return ECG_EARG;
+    CK(cudaStreamSynchronize(ctx->c.stream));
+    return ECG_OK;
+}
+
+}  // extern "C"

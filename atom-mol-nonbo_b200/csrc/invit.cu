@@ -1,0 +1,317 @@
+// invit.cu -- one inverse-iteration step and the Rayleigh quotient of
+// GHEPIIS (src/linalg.f90:1781-1926):
+//   w = B^H v                  MHMV, ZGEMV('C')         (src/linalg.f90:1019-1107)
+//   x = (L D L^H)^-1 w         LDLHS, 2 x ZTRSV + D^-1  (src/linalg.f90:618-775)
+//   x /= max|Re x|,|Im x|      CMaxAbsReOrIm + CVScale
+//   tc = x^H v / v^H v, NormOfDiff = sqrt(2n) ||x - tc v||
+//   t1 = x^H B x, t2 = x^H M x VMMHMV on the lower triangles
+//
+// The triangular solves walk the panels of the LDL^H factor.  Each panel
+// step is one launch whose CTAs share the dot products against the already
+// solved part; the last CTA to finish (atomic ticket, no waiting) sums the
+// partials in a fixed order and applies the panel's precomputed inverse
+// block, so results are deterministic run to run.
+#include "ecg_internal.h"
+
+namespace ecg {
+
+constexpr int SOLVE_G_MAX = 64;
+
+__device__ __forceinline__ cd ld2(const cd* p)
+{
+    const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+    return cd{v.x, v.y};
+}
+__device__ __forceinline__ cd ldcg2(const cd* p)
+{
+    const double2 v = __ldcg(reinterpret_cast<const double2*>(p));
+    return cd{v.x, v.y};
+}
+__device__ __forceinline__ cd warp_sum(cd s)
+{
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+        s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+    }
+    return s;
+}
+
+// w(i) = sum_j conj(B(j,i)) v(j); one warp per column, four accumulators.
+__global__ void __launch_bounds__(256) k_hemv(const cd* __restrict__ B, int ld, int n, const cd* __restrict__ v,
+                                              cd* __restrict__ w)
+{
+    const int col = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (col >= n) return;
+    const cd* b = B + (size_t)col * ld;
+    cd s0 = mk(0.0, 0.0), s1 = s0, s2 = s0, s3 = s0;
+    int j = lane;
+    for (; j + 96 < n; j += 128) {
+        const cd b0 = ld2(b + j), b1 = ld2(b + j + 32), b2 = ld2(b + j + 64), b3 = ld2(b + j + 96);
+        s0 = cfma(conj(b0), ld2(v + j), s0);
+        s1 = cfma(conj(b1), ld2(v + j + 32), s1);
+        s2 = cfma(conj(b2), ld2(v + j + 64), s2);
+        s3 = cfma(conj(b3), ld2(v + j + 96), s3);
+    }
+    for (; j < n; j += 32) s0 = cfma(conj(ld2(b + j)), ld2(v + j), s0);
+    const cd s = warp_sum((s0 + s1) + (s2 + s3));
+    if (lane == 0) w[col] = s;
+}
+
+// Forward solve of panel [j0, j1): y = Linv (w - U(0:j0, p)^H y(0:j0)),
+// z = invD y.  CTA g covers rows [g*chunk, ...) of the solved part.
+__global__ void __launch_bounds__(256) k_fwd(const cd* __restrict__ A, int ld, int j0, int j1, int chunk,
+                                             const cd* __restrict__ w, cd* __restrict__ y, cd* __restrict__ z,
+                                             const cd* __restrict__ invD, const cd* __restrict__ linv,
+                                             cd* __restrict__ part, int* __restrict__ counter)
+{
+    __shared__ cd t[LDL_NB];
+    __shared__ int last;
+    const int b = j1 - j0;
+    const int g = blockIdx.x, G = gridDim.x;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const int i0 = g * chunk, i1 = min(j0, i0 + chunk);
+    for (int m = wp; m < b; m += 8) {
+        const cd* col = A + (size_t)(j0 + m) * ld;
+        cd s = mk(0.0, 0.0);
+        for (int i = i0 + lane; i < i1; i += 32) s = cfma(conj(ld2(col + i)), ldcg2(y + i), s);
+        s = warp_sum(s);
+        if (lane == 0) part[g * LDL_NB + m] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(counter, 1) == G - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (threadIdx.x < b) {
+        cd s = mk(0.0, 0.0);
+        for (int q = 0; q < G; q++) s = s + ldcg2(part + q * LDL_NB + threadIdx.x);
+        t[threadIdx.x] = ld2(w + j0 + threadIdx.x) - s;
+    }
+    __syncthreads();
+    if (threadIdx.x < b) {
+        const int r = threadIdx.x;
+        const cd* Lr = linv + (size_t)(j0 + r) * LDL_NB;
+        cd s = mk(0.0, 0.0);
+        for (int q = 0; q <= r; q++) s = cfma(ld2(Lr + q), t[q], s);
+        y[j0 + r] = s;
+        z[j0 + r] = cmul(s, ld2(invD + j0 + r));
+    }
+    if (threadIdx.x == 0) *counter = 0;
+}
+
+// Backward solve of panel [j0, j1): x = Linv^H (z - U(p, j1:n) x(j1:n)).
+// CTA g covers columns [j1 + g*chunk, ...); 4 groups of 64 threads.
+__global__ void __launch_bounds__(256) k_bwd(const cd* __restrict__ A, int ld, int j0, int j1, int n, int chunk,
+                                             const cd* __restrict__ z, cd* __restrict__ x,
+                                             const cd* __restrict__ linv, cd* __restrict__ part,
+                                             int* __restrict__ counter)
+{
+    __shared__ cd sred[4][LDL_NB];
+    __shared__ cd t[LDL_NB];
+    __shared__ int last;
+    const int b = j1 - j0;
+    const int g = blockIdx.x, G = gridDim.x;
+    const int r = threadIdx.x & 63, grp = threadIdx.x >> 6;
+    const int c0 = j1 + g * chunk, c1 = min(n, c0 + chunk);
+    cd s = mk(0.0, 0.0);
+    if (r < b)
+        for (int c = c0 + grp; c < c1; c += 4) s = cfma(ld2(A + (size_t)(j0 + r) + (size_t)c * ld), ldcg2(x + c), s);
+    sred[grp][r] = s;
+    __syncthreads();
+    if (threadIdx.x < LDL_NB) {
+        const cd v = (sred[0][r] + sred[1][r]) + (sred[2][r] + sred[3][r]);
+        part[g * LDL_NB + r] = v;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(counter, 1) == G - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (threadIdx.x < b) {
+        cd q = mk(0.0, 0.0);
+        for (int k = 0; k < G; k++) q = q + ldcg2(part + k * LDL_NB + threadIdx.x);
+        t[threadIdx.x] = ld2(z + j0 + threadIdx.x) - q;
+    }
+    __syncthreads();
+    if (threadIdx.x < b) {
+        const int rr = threadIdx.x;
+        cd v = mk(0.0, 0.0);
+        for (int q = rr; q < b; q++) v = cfma(conj(ld2(linv + (size_t)(j0 + q) * LDL_NB + rr)), t[q], v);
+        x[j0 + rr] = v;
+    }
+    if (threadIdx.x == 0) *counter = 0;
+}
+
+// Block-wide deterministic sums (1024 threads).
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double* sh)
+{
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++)
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; k++) sh[wp * NV + k] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        double s = 0.0;
+        for (int q = 0; q < 32; q++) s += sh[q * NV + k];
+        v[k] = s;
+    }
+}
+
+// Normalisation and convergence measure of one step; ends with v <- x.
+__global__ void __launch_bounds__(1024) k_iter_norm(int n, cd* __restrict__ x, cd* __restrict__ v, double sqrtn,
+                                                    double* __restrict__ red)
+{
+    __shared__ double sh[32 * 3];
+    __shared__ double smax[32];
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    double m = 0.0;
+    for (int j = tid; j < n; j += 1024) {
+        const cd a = x[j];
+        m = fmax(m, fmax(fabs(a.x), fabs(a.y)));
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) smax[wp] = m;
+    __syncthreads();
+    double t1 = 0.0;
+    for (int q = 0; q < 32; q++) t1 = fmax(t1, smax[q]);
+    const double ra = 1.0 / t1;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int j = tid; j < n; j += 1024) {
+        cd a = x[j];
+        a = cd{ra * a.x, ra * a.y};
+        x[j] = a;
+        const cd b = v[j];
+        acc[0] = fma(a.x, b.x, fma(a.y, b.y, acc[0]));   // Re conj(x) v
+        acc[1] = fma(a.x, b.y, fma(-a.y, b.x, acc[1]));  // Im conj(x) v
+        acc[2] = fma(b.x, b.x, fma(b.y, b.y, acc[2]));
+    }
+    block_sum<3>(acc, sh);
+    const cd tc = cd{acc[0] / acc[2], acc[1] / acc[2]};
+    double d[1] = {0.0};
+    for (int j = tid; j < n; j += 1024) {
+        const cd a = x[j];
+        const cd s = cfms(tc, v[j], a);
+        d[0] = fma(s.x, s.x, fma(s.y, s.y, d[0]));
+    }
+    __syncthreads();
+    block_sum<1>(d, sh);
+    if (tid == 0) red[RD_NORMDIFF] = sqrtn * sqrt(d[0]);
+    __syncthreads();
+    for (int j = tid; j < n; j += 1024) v[j] = x[j];
+}
+
+// Per-column terms of x^H A x over the lower triangle (VMMHMV,
+// src/linalg.f90:1195-1206) for A = B (blockIdx.y = 0) and A = M (1).
+__global__ void __launch_bounds__(256) k_vmm_cols(const cd* __restrict__ B, const cd* __restrict__ M, int ld, int n,
+                                                  const cd* __restrict__ x, double* __restrict__ colval)
+{
+    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (k >= n) return;
+    const cd* A = (blockIdx.y == 0) ? B : M;
+    const cd* col = A + (size_t)k * ld;
+    double sr = 0.0, si = 0.0;
+    for (int j = k + 1 + lane; j < n; j += 32) {
+        const cd a = ld2(col + j), xj = ld2(x + j);
+        sr = fma(xj.x, a.x, fma(xj.y, a.y, sr));
+        si = fma(xj.y, a.x, fma(-xj.x, a.y, si));
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+        si += __shfl_xor_sync(0xffffffffu, si, o);
+    }
+    if (lane == 0) {
+        const cd xk = ld2(x + k);
+        const double dk = ld2(col + k).x;
+        colval[(size_t)blockIdx.y * n + k] = fma(xk.x * xk.x + xk.y * xk.y, dk, 2.0 * (xk.x * sr + xk.y * si));
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_vmm_reduce(int n, const double* __restrict__ colval,
+                                                     const cd* __restrict__ x, double* __restrict__ red)
+{
+    __shared__ double sh[32 * 3];
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int j = threadIdx.x; j < n; j += 1024) {
+        acc[0] += colval[j];
+        acc[1] += colval[n + j];
+        const cd a = x[j];
+        acc[2] = fma(a.x, a.x, fma(a.y, a.y, acc[2]));
+    }
+    block_sum<3>(acc, sh);
+    if (threadIdx.x == 0) {
+        red[RD_T1] = acc[0];
+        red[RD_T2] = acc[1];
+        red[RD_XX] = acc[2];
+    }
+}
+
+__global__ void k_vec_scale(cd* __restrict__ v, int n, double s)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) {
+        const cd a = v[j];
+        v[j] = cd{s * a.x, s * a.y};
+    }
+}
+
+// ---------------------------------------------------------------------------
+int invit_step(Ctx& c, int n, bool /*first*/)
+{
+    k_hemv<<<(n * 32 + 255) / 256, 256, 0, c.stream>>>(c.S, c.ld, n, c.c, c.w);
+    c.launches++;
+    const int nb = (int)c.blk_start.size();
+    for (int i = 0; i < nb; i++) {
+        const int j0 = c.blk_start[i], j1 = (i + 1 < nb) ? c.blk_start[i + 1] : n;
+        int G = (j0 + 127) / 128;
+        G = G < 1 ? 1 : (G > SOLVE_G_MAX ? SOLVE_G_MAX : G);
+        const int chunk = (j0 + G - 1) / G;
+        k_fwd<<<G, 256, 0, c.stream>>>(c.H, c.ld, j0, j1, chunk > 0 ? chunk : 1, c.w, c.yv, c.zv, c.invD, c.linv,
+                                      c.spart, c.counters);
+        c.launches++;
+    }
+    for (int i = nb - 1; i >= 0; i--) {
+        const int j0 = c.blk_start[i], j1 = (i + 1 < nb) ? c.blk_start[i + 1] : n;
+        const int rest = n - j1;
+        int G = (rest + 127) / 128;
+        G = G < 1 ? 1 : (G > SOLVE_G_MAX ? SOLVE_G_MAX : G);
+        const int chunk = (rest + G - 1) / G;
+        k_bwd<<<G, 256, 0, c.stream>>>(c.H, c.ld, j0, j1, n, chunk > 0 ? chunk : 1, c.zv, c.x, c.linv, c.spart,
+                                      c.counters + 1);
+        c.launches++;
+    }
+    k_iter_norm<<<1, 1024, 0, c.stream>>>(n, c.x, c.c, sqrt(2.0 * n), c.red);
+    c.launches++;
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int invit_rayleigh(Ctx& c, int n)
+{
+    dim3 g((n * 32 + 255) / 256, 2);
+    k_vmm_cols<<<g, 256, 0, c.stream>>>(c.S, c.H, c.ld, n, c.x, c.colval);
+    k_vmm_reduce<<<1, 1024, 0, c.stream>>>(n, c.colval, c.x, c.red);
+    c.launches += 2;
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int vec_scale(Ctx& c, cd* v, int n, double s)
+{
+    k_vec_scale<<<(n + 255) / 256, 256, 0, c.stream>>>(v, n, s);
+    c.launches++;
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+}  // namespace ecg

@@ -1,0 +1,784 @@
+// pair_kernels.cu -- symmetry-projected pair elements over the lower
+// triangle of the basis, fused with their normalised store.
+//
+//   k_prep          per-function data: Ck = A - iB (bra), P'AP + iP'BP per
+//                   Y^+Y term (ket), det L           (src/matelem.f90:109-194)
+//   k_pair_diag     diagonal pairs + StoreHS/StoreHSD diagonal branch
+//                   (src/matform.f90:22-25, 36-39, 84-88)
+//   k_pair_energy   off-diagonal pairs, sum over Y^+Y terms, StoreHS
+//                   (src/matform.f90:119-230 with :26-35, :40-49)
+//   k_pair_grad     off-diagonal pairs with derivatives, StoreHSD
+//                   (src/matform.f90:234-360 with :89-114)
+//   k_adjoint       dE/dp contracted per pair and reduced per function,
+//                   replacing Glob_D and the loop of src/workproc.f90:2127-2142
+//   k_contract      the loop of src/workproc.f90:2127-2142 over Glob_D
+//
+// Grid shape: one CTA per 32 x 32 tile of the lower triangle; lanes run
+// along the row index k (the contiguous index of the column-major H and S),
+// warps along the column index l.
+#include "ecg_internal.h"
+#include "ecg_grad.cuh"
+
+namespace ecg {
+
+__device__ __forceinline__ cd ldcd(const cd* p)
+{
+    const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+    return cd{v.x, v.y};
+}
+__device__ __forceinline__ void stcd(cd* p, cd v) { *reinterpret_cast<double2*>(p) = make_double2(v.x, v.y); }
+
+template <int N>
+__device__ __forceinline__ void load_sym(const cd* __restrict__ p, cd (&M)[N][N])
+{
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+        for (int j = i; j < N; j++) {
+            const cd v = ldcd(p + vech_index(N, i, j));
+            M[j][i] = v;
+            M[i][j] = v;
+        }
+}
+
+template <int N>
+__device__ __forceinline__ void load_L(const double* __restrict__ p, double (&L)[N][N])
+{
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+        for (int j = i; j < N; j++) {
+            L[i][j] = 0.0;
+            L[j][i] = __ldg(p + vech_index(N, i, j));
+        }
+}
+
+template <int N>
+__device__ __forceinline__ void load_P(const double* __restrict__ Pd, int t, double (&P)[N][N])
+{
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+        for (int j = 0; j < N; j++) P[i][j] = Pd[(t * NMAX + i) * NMAX + j];
+}
+
+// L L' exactly as src/matelem.f90:124-139 (sum over k = 1..j).
+template <int N>
+__device__ __forceinline__ void gram(const double (&L)[N][N], double (&A)[N][N])
+{
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+        for (int j = i; j < N; j++) {
+            double r = 0.0;
+#pragma unroll
+            for (int k = 0; k <= j; k++) r = fma(L[i][k], L[j][k], r);
+            A[i][j] = r;
+            A[j][i] = r;
+        }
+}
+
+template <int N>
+__device__ __forceinline__ void sym_from_vech(const double* __restrict__ p, double (&B)[N][N])
+{
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+        for (int j = i; j < N; j++) {
+            const double v = __ldg(p + vech_index(N, i, j));
+            B[i][j] = v;
+            B[j][i] = v;
+        }
+}
+
+// P' X P for symmetric X (src/matelem.f90:144-169); products with the 0/+-1
+// entries of P are exact, so the result does not depend on FMA contraction.
+template <int N>
+__device__ __forceinline__ void perm_sym(const double (&P)[N][N], const double (&X)[N][N], double (&Y)[N][N])
+{
+    double W[N][N];
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+            double r = 0.0;
+#pragma unroll
+            for (int k = 0; k < N; k++) r = fma(P[k][i], X[k][j], r);
+            W[i][j] = r;
+        }
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+        for (int j = i; j < N; j++) {
+            double r = 0.0;
+#pragma unroll
+            for (int k = 0; k < N; k++) r = fma(W[i][k], P[k][j], r);
+            Y[i][j] = r;
+            Y[j][i] = r;
+        }
+}
+
+// bra data of one function: Ck = A - iB and det L
+template <int N>
+__device__ __forceinline__ void make_bra(const double* __restrict__ p, cd (&Ck)[N][N], double& det)
+{
+    constexpr int NP = Sym<N>::NP;
+    double L[N][N], A[N][N], B[N][N];
+    load_L<N>(p, L);
+    gram<N>(L, A);
+    sym_from_vech<N>(p + NP, B);
+    det = 1.0;
+#pragma unroll
+    for (int i = 0; i < N; i++) det *= L[i][i];
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+        for (int j = 0; j < N; j++) Ck[i][j] = mk(A[i][j], -B[i][j]);
+}
+
+// ket data of one function under one permutation: tCl = P'AP + iP'BP
+template <int N>
+__device__ __forceinline__ void make_ket(const double* __restrict__ p, const double (&P)[N][N], cd (&tCl)[N][N],
+                                         double& det)
+{
+    constexpr int NP = Sym<N>::NP;
+    double L[N][N], A[N][N], B[N][N], tA[N][N], tB[N][N];
+    load_L<N>(p, L);
+    gram<N>(L, A);
+    sym_from_vech<N>(p + NP, B);
+    perm_sym<N>(P, A, tA);
+    perm_sym<N>(P, B, tB);
+    det = 1.0;
+#pragma unroll
+    for (int i = 0; i < N; i++) det *= L[i][i];
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+        for (int j = 0; j < N; j++) tCl[i][j] = mk(tA[i][j], tB[i][j]);
+}
+
+template <int N>
+__device__ __forceinline__ void store_sym(cd* p, const cd (&M)[N][N])
+{
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+        for (int j = i; j < N; j++) stcd(p + vech_index(N, i, j), M[j][i]);
+}
+
+// ---------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(128) k_prep(const double* __restrict__ params, const double* __restrict__ Pd,
+                                              int T, int nfun, cd* __restrict__ bra, cd* __restrict__ ket,
+                                              double* __restrict__ detL)
+{
+    constexpr int NP = Sym<N>::NP;
+    constexpr int NPT = 2 * NP;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nfun) return;
+    const double* p = params + (size_t)f * NPT;
+    cd Ck[N][N];
+    double det;
+    make_bra<N>(p, Ck, det);
+    store_sym<N>(bra + (size_t)f * NP, Ck);
+    detL[f] = det;
+    for (int t = 0; t < T; t++) {
+        double P[N][N];
+        load_P<N>(Pd, t, P);
+        cd tCl[N][N];
+        double d2;
+        make_ket<N>(p, P, tCl, d2);
+        store_sym<N>(ket + ((size_t)f * T + t) * NP, tCl);
+    }
+}
+
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void tile_rc(long long b, int Rlo, int& R, int& C)
+{
+    const long long bb = b + (long long)Rlo * (Rlo + 1) / 2;
+    long long r = (long long)((sqrt(8.0 * (double)bb + 1.0) - 1.0) * 0.5);
+    while (r * (r + 1) / 2 > bb) r--;
+    while ((r + 1) * (r + 2) / 2 <= bb) r++;
+    R = (int)r;
+    C = (int)(bb - r * (r + 1) / 2);
+}
+
+// Diagonal pairs k = l for k in [r0, r1).  deriv: also Glob_D(:,k-nfru,k).
+template <int N, bool DERIV>
+__global__ void __launch_bounds__(128) k_pair_diag(SysParams sp, const double* __restrict__ coef,
+                                                   const double* __restrict__ Pd, const double* __restrict__ params,
+                                                   const cd* __restrict__ bra, const cd* __restrict__ ket,
+                                                   const double* __restrict__ detL, double* __restrict__ diagS,
+                                                   double* __restrict__ diagH, cd* __restrict__ H, cd* __restrict__ S,
+                                                   int ld, int r0, int r1, char method, double approx_e,
+                                                   cd* __restrict__ D, int ldo, int nfru)
+{
+    constexpr int NP = Sym<N>::NP;
+    const int k = r0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= r1) return;
+    cd Ck[N][N];
+    load_sym<N>(bra + (size_t)k * NP, Ck);
+    const double dk = detL[k];
+    const double absdet = fabs(dk * dk);
+    cd Hs = mk(0.0, 0.0), Ss = mk(0.0, 0.0);
+    cd Dks[4 * NP];
+    double Lk[N][N];
+    if (DERIV) {
+        load_L<N>(params + (size_t)k * 2 * NP, Lk);
+#pragma unroll
+        for (int m = 0; m < 4 * NP; m++) Dks[m] = mk(0.0, 0.0);
+    }
+    for (int t = 0; t < sp.T; t++) {
+        cd tCl[N][N];
+        load_sym<N>(ket + ((size_t)k * sp.T + t) * NP, tCl);
+        TermEnergy<N> te;
+        term_energy<N>(Ck, tCl, absdet, sp, te);
+        const double cf = coef[t];
+        Hs = rfma(cf, te.T + te.V, Hs);
+        Ss = rfma(cf, te.S, Ss);
+        if (DERIV) {
+            double P[N][N];
+            load_P<N>(Pd, t, P);
+            cd Dk[4 * NP], Dl[1];
+            term_grad_plain<N, true, false>(Lk, Lk, P, Ck, tCl, te, sp, Dk, Dl);
+#pragma unroll
+            for (int m = 0; m < 4 * NP; m++) Dks[m] = rfma(cf, Dk[m], Dks[m]);
+        }
+    }
+    const double dS = Ss.x;
+    diagS[k] = dS;
+    const size_t kk = (size_t)k + (size_t)k * ld;
+    if (method == 'I') {
+        S[kk] = mk(1.0, 0.0);
+        H[kk] = mk(Hs.x / dS - approx_e, 0.0);
+    } else {
+        diagH[k] = Hs.x / dS;
+    }
+    if (DERIV) {
+        cd* d = D + ((size_t)(k - nfru) + (size_t)k * ldo) * (4 * NP);
+#pragma unroll
+        for (int m = 0; m < 4 * NP; m++) d[m] = mk(2.0 * Dks[m].x / dS, 0.0);
+    }
+}
+
+// Off-diagonal pairs k > l, k in [r0, r1): H, S only.
+template <int N>
+__global__ void __launch_bounds__(256) k_pair_energy(SysParams sp, const double* __restrict__ coef,
+                                                     const cd* __restrict__ bra, const cd* __restrict__ ket,
+                                                     const double* __restrict__ detL,
+                                                     const double* __restrict__ diagS, cd* __restrict__ H,
+                                                     cd* __restrict__ S, int ld, int r0, int r1, int Rlo,
+                                                     char method, double approx_e)
+{
+    constexpr int NP = Sym<N>::NP;
+    int R, C;
+    tile_rc(blockIdx.x, Rlo, R, C);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int k = R * TILE + lane;
+    if (k < r0 || k >= r1) return;
+    cd Ck[N][N];
+    load_sym<N>(bra + (size_t)k * NP, Ck);
+    const double dk = detL[k];
+    const double dSk = diagS[k];
+#pragma unroll 1
+    for (int j = 0; j < TILE / 8; j++) {
+        const int l = C * TILE + w + 8 * j;
+        if (l >= k) break;
+        const double absdet = fabs(detL[l] * dk);
+        cd Hs = mk(0.0, 0.0), Ss = mk(0.0, 0.0);
+#pragma unroll 1
+        for (int t = 0; t < sp.T; t++) {
+            cd tCl[N][N];
+            load_sym<N>(ket + ((size_t)l * sp.T + t) * NP, tCl);
+            TermEnergy<N> te;
+            term_energy<N>(Ck, tCl, absdet, sp, te);
+            const double cf = __ldg(coef + t);
+            Hs = rfma(cf, te.T + te.V, Hs);
+            Ss = rfma(cf, te.S, Ss);
+        }
+        const double f = 1.0 / sqrt(dSk * diagS[l]);
+        const size_t kl = (size_t)k + (size_t)l * ld;
+        const cd s = f * Ss;
+        S[kl] = s;
+        if (method == 'I') {
+            S[(size_t)l + (size_t)k * ld] = conj(s);
+            H[kl] = f * (Hs - approx_e * Ss);
+        } else {
+            H[kl] = f * Hs;
+        }
+    }
+}
+
+// Off-diagonal pairs with derivatives, one pair per thread at a time; the
+// per-term derivative sums live in shared memory ([value][thread]).
+template <int N, int NT>
+__global__ void __launch_bounds__(NT) k_pair_grad(SysParams sp, const double* __restrict__ coef,
+                                                  const double* __restrict__ Pd,
+                                                  const double* __restrict__ params, const cd* __restrict__ bra,
+                                                  const cd* __restrict__ ket, const double* __restrict__ detL,
+                                                  const double* __restrict__ diagS, cd* __restrict__ H,
+                                                  cd* __restrict__ S, int ld, int r0, int r1, int Rlo, char method,
+                                                  double approx_e, cd* __restrict__ D, int ldo, int nfru)
+{
+    constexpr int NP = Sym<N>::NP;
+    constexpr int NV = 8 * NP;  // complex values: Dk (4NP) + Dl (4NP)
+    extern __shared__ double acc[];
+    int R, C;
+    tile_rc(blockIdx.x, Rlo, R, C);
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, w = tid >> 5;
+    constexpr int NW = NT / 32;
+    const int k = R * TILE + lane;
+    if (k < r0 || k >= r1) return;
+    cd Ck[N][N];
+    load_sym<N>(bra + (size_t)k * NP, Ck);
+    double Lk[N][N];
+    load_L<N>(params + (size_t)k * 2 * NP, Lk);
+    const double dk = detL[k];
+    const double dSk = diagS[k];
+    auto A = [&](int v) -> double& { return acc[v * NT + tid]; };
+#pragma unroll 1
+    for (int j = 0; j < TILE / NW; j++) {
+        const int l = C * TILE + w + NW * j;
+        if (l >= k) break;
+        const bool gl = (l >= nfru);
+        double Ll[N][N];
+        load_L<N>(params + (size_t)l * 2 * NP, Ll);
+        const double absdet = fabs(detL[l] * dk);
+        for (int v = 0; v < 2 * NV; v++) A(v) = 0.0;
+        cd Hs = mk(0.0, 0.0), Ss = mk(0.0, 0.0);
+#pragma unroll 1
+        for (int t = 0; t < sp.T; t++) {
+            cd tCl[N][N];
+            load_sym<N>(ket + ((size_t)l * sp.T + t) * NP, tCl);
+            TermEnergy<N> te;
+            term_energy<N>(Ck, tCl, absdet, sp, te);
+            const double cf = __ldg(coef + t);
+            Hs = rfma(cf, te.T + te.V, Hs);
+            Ss = rfma(cf, te.S, Ss);
+            double P[N][N];
+            load_P<N>(Pd, t, P);
+            cd Dk[4 * NP], Dl[4 * NP];
+            if (gl) {
+                term_grad_plain<N, true, true>(Lk, Ll, P, Ck, tCl, te, sp, Dk, Dl);
+#pragma unroll
+                for (int m = 0; m < 4 * NP; m++) {
+                    A(2 * (4 * NP + m)) = fma(cf, Dl[m].x, A(2 * (4 * NP + m)));
+                    A(2 * (4 * NP + m) + 1) = fma(cf, Dl[m].y, A(2 * (4 * NP + m) + 1));
+                }
+            } else {
+                term_grad_plain<N, true, false>(Lk, Ll, P, Ck, tCl, te, sp, Dk, Dl);
+            }
+#pragma unroll
+            for (int m = 0; m < 4 * NP; m++) {
+                A(2 * m) = fma(cf, Dk[m].x, A(2 * m));
+                A(2 * m + 1) = fma(cf, Dk[m].y, A(2 * m + 1));
+            }
+        }
+        const double f = 1.0 / sqrt(dSk * diagS[l]);
+        const size_t kl = (size_t)k + (size_t)l * ld;
+        const cd s = f * Ss;
+        S[kl] = s;
+        if (method == 'I') {
+            S[(size_t)l + (size_t)k * ld] = conj(s);
+            H[kl] = f * (Hs - approx_e * Ss);
+        } else {
+            H[kl] = f * Hs;
+        }
+        cd* dkl = D + ((size_t)(k - nfru) + (size_t)l * ldo) * (4 * NP);
+        for (int m = 0; m < 4 * NP; m++) stcd(dkl + m, mk(f * A(2 * m), f * A(2 * m + 1)));
+        if (gl) {
+            cd* dlk = D + ((size_t)(l - nfru) + (size_t)k * ldo) * (4 * NP);
+            for (int m = 0; m < 4 * NP; m++)
+                stcd(dlk + m, mk(f * A(2 * (4 * NP + m)), -f * A(2 * (4 * NP + m) + 1)));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint gradient.  For pair (k >= l) with weight w = conj(c_k) c_l f_kl:
+//   row function k   gets  w * sum_t coef_t Z_k(t)        and Re(w a)
+//   column function l gets conj(w * sum_t coef_t Z_l(t))  and Re(w a)
+//   (column part only for k != l and l > nfru).
+// Per tile, rows are reduced over the 8 warps and columns over the 32 lanes
+// (butterfly), and written to part[tile][side][slot][NV] in a fixed order.
+// ---------------------------------------------------------------------------
+template <int N>
+struct AdjNV {
+    static constexpr int value = 2 * Sym<N>::NP + 1;
+};
+
+template <int N>
+__global__ void __launch_bounds__(256) k_adjoint(SysParams sp, const double* __restrict__ coef,
+                                                 const double* __restrict__ Pd, const cd* __restrict__ bra,
+                                                 const cd* __restrict__ ket, const double* __restrict__ detL,
+                                                 const double* __restrict__ diagS, const cd* __restrict__ cvec,
+                                                 double E, int nfru, int nfa, int Rlo, double* __restrict__ part)
+{
+    constexpr int NP = Sym<N>::NP;
+    constexpr int NV = AdjNV<N>::value;
+    extern __shared__ double red[];  // [8][32][NV]
+    int R, C;
+    tile_rc(blockIdx.x, Rlo, R, C);
+    const long long tile = blockIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int k = R * TILE + lane;
+    const bool krow = (k >= nfru && k < nfa);
+    cd Ck[N][N];
+    double dk = 1.0, dSk = 1.0;
+    cd ck = mk(0.0, 0.0);
+    if (krow) {
+        load_sym<N>(bra + (size_t)k * NP, Ck);
+        dk = detL[k];
+        dSk = diagS[k];
+        ck = ldcd(cvec + k);
+    }
+    cd Ak[NP];
+    double dl_k = 0.0;
+#pragma unroll
+    for (int x = 0; x < NP; x++) Ak[x] = mk(0.0, 0.0);
+#pragma unroll 1
+    for (int j = 0; j < TILE / 8; j++) {
+        const int l = C * TILE + w + 8 * j;
+        const bool valid = krow && (l <= k);
+        const bool ketw = (l >= nfru);  // warp-uniform
+        cd Zk[NP], Zl[NP], a = mk(0.0, 0.0);
+#pragma unroll
+        for (int x = 0; x < NP; x++) {
+            Zk[x] = mk(0.0, 0.0);
+            Zl[x] = mk(0.0, 0.0);
+        }
+        cd wkl = mk(0.0, 0.0);
+        if (valid) {
+            const double absdet = fabs(detL[l] * dk);
+#pragma unroll 1
+            for (int t = 0; t < sp.T; t++) {
+                cd tCl[N][N];
+                load_sym<N>(ket + ((size_t)l * sp.T + t) * NP, tCl);
+                TermEnergy<N> te;
+                term_energy<N>(Ck, tCl, absdet, sp, te);
+                double P[N][N];
+                load_P<N>(Pd, t, P);
+                const double cf = __ldg(coef + t);
+                if (ketw)
+                    term_adjoint<N, true>(P, Ck, tCl, te, sp, E, cf, Zk, Zl, a);
+                else
+                    term_adjoint<N, false>(P, Ck, tCl, te, sp, E, cf, Zk, Zl, a);
+            }
+            const double f = 1.0 / sqrt(dSk * diagS[l]);
+            wkl = f * cmul(conj(ck), ldcd(cvec + l));
+        }
+        const double ra = cmul(wkl, a).x;
+#pragma unroll
+        for (int x = 0; x < NP; x++) Ak[x] = cfma(wkl, Zk[x], Ak[x]);
+        dl_k += ra;
+        if (ketw) {
+            const bool kc = valid && (l != k);
+            double v[NV];
+#pragma unroll
+            for (int x = 0; x < NP; x++) {
+                const cd z = kc ? conj(cmul(wkl, Zl[x])) : mk(0.0, 0.0);
+                v[2 * x] = z.x;
+                v[2 * x + 1] = z.y;
+            }
+            v[NV - 1] = kc ? ra : 0.0;
+#pragma unroll
+            for (int s = 16; s >= 1; s >>= 1)
+#pragma unroll
+                for (int x = 0; x < NV; x++) v[x] += __shfl_xor_sync(0xffffffffu, v[x], s);
+            if (lane == 0) {
+                double* dst = part + ((tile * 2 + 1) * TILE + (w + 8 * j)) * NV;
+#pragma unroll
+                for (int x = 0; x < NV; x++) dst[x] = v[x];
+            }
+        }
+    }
+    double* r = red + ((size_t)w * TILE + lane) * NV;
+#pragma unroll
+    for (int x = 0; x < NP; x++) {
+        r[2 * x] = Ak[x].x;
+        r[2 * x + 1] = Ak[x].y;
+    }
+    r[NV - 1] = dl_k;
+    __syncthreads();
+    if (w == 0) {
+        double* dst = part + ((tile * 2 + 0) * TILE + lane) * NV;
+        for (int x = 0; x < NV; x++) {
+            double s = 0.0;
+#pragma unroll
+            for (int q = 0; q < 8; q++) s += red[((size_t)q * TILE + lane) * NV + x];
+            dst[x] = s;
+        }
+    }
+}
+
+// One warp per function f in [nfru, nfa): sum its row and column partials
+// in a fixed order and form dE/d(vech L_f, vech B_f).
+template <int N>
+__global__ void __launch_bounds__(256) k_adjoint_final(const double* __restrict__ part,
+                                                       const double* __restrict__ params, int nfru, int nfa,
+                                                       int Rlo, int nR, double* __restrict__ grad)
+{
+    constexpr int NP = Sym<N>::NP;
+    constexpr int NV = AdjNV<N>::value;
+    const int lane = threadIdx.x & 31;
+    const int f = nfru + (blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    if (f >= nfa) return;
+    const int Rf = f / TILE, slot = f % TILE;
+    const long long base = (long long)Rlo * (Rlo + 1) / 2;
+    double v[NV];
+#pragma unroll
+    for (int x = 0; x < NV; x++) v[x] = 0.0;
+    for (int Cc = lane; Cc <= Rf; Cc += 32) {
+        const long long t = (long long)Rf * (Rf + 1) / 2 - base + Cc;
+        const double* src = part + ((t * 2 + 0) * TILE + slot) * NV;
+#pragma unroll
+        for (int x = 0; x < NV; x++) v[x] += src[x];
+    }
+    for (int Rr = Rf + lane; Rr < nR; Rr += 32) {
+        const long long t = (long long)Rr * (Rr + 1) / 2 - base + Rf;
+        const double* src = part + ((t * 2 + 1) * TILE + slot) * NV;
+#pragma unroll
+        for (int x = 0; x < NV; x++) v[x] += src[x];
+    }
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1)
+#pragma unroll
+        for (int x = 0; x < NV; x++) v[x] += __shfl_xor_sync(0xffffffffu, v[x], s);
+    if (lane < NP) {
+        // vech entry x = (column i, row j >= i)
+        int i = 0, x = lane;
+        while (x >= N - i) {
+            x -= N - i;
+            i++;
+        }
+        const int j = i + x;
+        const double* p = params + (size_t)f * 2 * NP;
+        double acc = 0.0;
+        for (int m = i; m < N; m++) {
+            // A(j,m) from the packed lower triangle, L(m,i) = vech(i,m)
+            const int a = (j >= m) ? vech_index(N, m, j) : vech_index(N, j, m);
+            acc += v[2 * a] * p[vech_index(N, i, m)];
+        }
+        double gL = -4.0 * acc;
+        if (i == j) gL += 2.0 * v[NV - 1] / p[vech_index(N, i, i)];
+        const int a = vech_index(N, i, j);
+        const double gB = -2.0 * ((i == j) ? 1.0 : 2.0) * v[2 * a + 1];
+        double* g = grad + (size_t)(f - nfru) * 2 * NP;
+        g[lane] = gL;
+        g[NP + lane] = gB;
+    }
+}
+
+// Contraction of Glob_D, src/workproc.f90:2127-2142: one CTA per function.
+__global__ void __launch_bounds__(256) k_contract(const cd* __restrict__ D, int ldo, int npt,
+                                                  const cd* __restrict__ cvec, double E, int nfo, int nfa,
+                                                  int nfru, double* __restrict__ grad)
+{
+    __shared__ double sw[8][32][2];
+    const int k = blockIdx.x;  // 0-based row of Glob_D's second index
+    if (k >= nfo) return;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int n2 = 2 * npt;
+    cd W = mk(0.0, 0.0);
+    if (lane < npt) {
+        for (int l = w; l < nfa; l += 8) {
+            const cd* d = D + ((size_t)k + (size_t)l * ldo) * n2;
+            const cd t = ldcd(cvec + l);
+            const cd dh = ldcd(d + lane), ds = ldcd(d + npt + lane);
+            W = cfma(t, dh - E * ds, W);
+        }
+    }
+    sw[w][lane][0] = W.x;
+    sw[w][lane][1] = W.y;
+    __syncthreads();
+    if (w == 0 && lane < npt) {
+        cd s = mk(0.0, 0.0);
+        for (int q = 0; q < 8; q++) s = s + mk(sw[q][lane][0], sw[q][lane][1]);
+        const cd t = ldcd(cvec + k + nfru);
+        const cd* d = D + ((size_t)k + (size_t)(k + nfru) * ldo) * n2;
+        const cd dd = ldcd(d + lane) - E * ldcd(d + npt + lane);
+        double g = 2.0 * cmul(conj(t), s).x;
+        g = g - cmul(cmul(t, conj(t)), dd).x;
+        grad[(size_t)k * npt + lane] = g;
+    }
+}
+
+// One MatrixElements call per thread (explicit bra/ket parameters, term t).
+template <int N>
+__global__ void __launch_bounds__(128) k_term_batch(SysParams sp, const double* __restrict__ Pd, int count,
+                                                    const double* __restrict__ pk, const double* __restrict__ pl,
+                                                    const int* __restrict__ term, int gradflag, cd* __restrict__ hs,
+                                                    cd* __restrict__ dko, cd* __restrict__ dlo)
+{
+    constexpr int NP = Sym<N>::NP;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const double* a = pk + (size_t)i * 2 * NP;
+    const double* b = pl + (size_t)i * 2 * NP;
+    double P[N][N];
+    load_P<N>(Pd, term[i], P);
+    cd Ck[N][N], tCl[N][N];
+    double dk, dl;
+    make_bra<N>(a, Ck, dk);
+    make_ket<N>(b, P, tCl, dl);
+    TermEnergy<N> te;
+    term_energy<N>(Ck, tCl, fabs(dl * dk), sp, te);
+    hs[2 * (size_t)i] = te.T + te.V;
+    hs[2 * (size_t)i + 1] = te.S;
+    if (gradflag < 1 || gradflag > 3) return;
+    double Lk[N][N], Ll[N][N];
+    load_L<N>(a, Lk);
+    load_L<N>(b, Ll);
+    cd Dk[4 * NP], Dl[4 * NP];
+    if (gradflag == 1)
+        term_grad_plain<N, true, false>(Lk, Ll, P, Ck, tCl, te, sp, Dk, Dl);
+    else if (gradflag == 2)
+        term_grad_plain<N, false, true>(Lk, Ll, P, Ck, tCl, te, sp, Dk, Dl);
+    else
+        term_grad_plain<N, true, true>(Lk, Ll, P, Ck, tCl, te, sp, Dk, Dl);
+    if (gradflag & 1)
+        for (int m = 0; m < 4 * NP; m++) dko[(size_t)i * 4 * NP + m] = Dk[m];
+    if (gradflag & 2)
+        for (int m = 0; m < 4 * NP; m++) dlo[(size_t)i * 4 * NP + m] = Dl[m];
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+#define ECG_DISPATCH_N(n, FN, ...)              \
+    switch (n) {                                \
+        case 2: return FN<2>(__VA_ARGS__);      \
+        case 3: return FN<3>(__VA_ARGS__);      \
+        case 4: return FN<4>(__VA_ARGS__);      \
+        case 5: return FN<5>(__VA_ARGS__);      \
+        default: return -1;                     \
+    }
+
+static int last_err() { return cudaGetLastError() == cudaSuccess ? 0 : -2; }
+
+template <int N>
+static int prep_n(Ctx& c, int nfun)
+{
+    if (nfun <= 0) return 0;
+    k_prep<N><<<(nfun + 127) / 128, 128, 0, c.stream>>>(c.params, c.Pd, c.T, nfun, c.bra, c.ket, c.detL);
+    c.launches++;
+    return last_err();
+}
+int launch_prep(Ctx& c, int nfun) { ECG_DISPATCH_N(c.n, prep_n, c, nfun) }
+
+template <int N>
+static int diag_n(Ctx& c, int r0, int r1, double approx_e, int deriv, int nfru)
+{
+    if (r1 <= r0) return 0;
+    const int nb = (r1 - r0 + 127) / 128;
+    if (deriv)
+        k_pair_diag<N, true><<<nb, 128, 0, c.stream>>>(c.sp, c.coef, c.Pd, c.params, c.bra, c.ket, c.detL, c.diagS,
+                                                       c.diagH, c.H, c.S, c.ld, r0, r1, c.method, approx_e, c.D,
+                                                       c.max_nfo, nfru);
+    else
+        k_pair_diag<N, false><<<nb, 128, 0, c.stream>>>(c.sp, c.coef, c.Pd, c.params, c.bra, c.ket, c.detL,
+                                                        c.diagS, c.diagH, c.H, c.S, c.ld, r0, r1, c.method,
+                                                        approx_e, c.D, c.max_nfo, nfru);
+    c.launches++;
+    return last_err();
+}
+int launch_pair_diag(Ctx& c, int r0, int r1, double approx_e, int deriv, int nfru)
+{
+    ECG_DISPATCH_N(c.n, diag_n, c, r0, r1, approx_e, deriv, nfru)
+}
+
+template <int N>
+static int energy_n(Ctx& c, int r0, int r1, double approx_e)
+{
+    if (r1 <= r0) return 0;
+    const int Rlo = r0 / TILE, Rhi = (r1 + TILE - 1) / TILE;
+    const long long nt = tile_count(Rlo, Rhi);
+    k_pair_energy<N><<<(unsigned)nt, 256, 0, c.stream>>>(c.sp, c.coef, c.bra, c.ket, c.detL, c.diagS, c.H, c.S,
+                                                         c.ld, r0, r1, Rlo, c.method, approx_e);
+    c.launches++;
+    return last_err();
+}
+int launch_pair_energy(Ctx& c, int r0, int r1, double approx_e) { ECG_DISPATCH_N(c.n, energy_n, c, r0, r1, approx_e) }
+
+template <int N>
+static int grad_n(Ctx& c, int r0, int r1, int nfru, double approx_e)
+{
+    if (r1 <= r0) return 0;
+    constexpr int NT = (N <= 4) ? 128 : 64;
+    constexpr int NP = Sym<N>::NP;
+    const size_t smem = (size_t)16 * NP * NT * sizeof(double);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_pair_grad<N, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    const int Rlo = r0 / TILE, Rhi = (r1 + TILE - 1) / TILE;
+    const long long nt = tile_count(Rlo, Rhi);
+    k_pair_grad<N, NT><<<(unsigned)nt, NT, smem, c.stream>>>(c.sp, c.coef, c.Pd, c.params, c.bra, c.ket, c.detL,
+                                                             c.diagS, c.H, c.S, c.ld, r0, r1, Rlo, c.method,
+                                                             approx_e, c.D, c.max_nfo, nfru);
+    c.launches++;
+    return last_err();
+}
+int launch_pair_plain_grad(Ctx& c, int r0, int r1, int nfru, double approx_e)
+{
+    ECG_DISPATCH_N(c.n, grad_n, c, r0, r1, nfru, approx_e)
+}
+
+template <int N>
+static int adjoint_n(Ctx& c, int nfru, int nfa, double E)
+{
+    if (nfa <= nfru) return 0;
+    constexpr int NV = AdjNV<N>::value;
+    const int Rlo = nfru / TILE, Rhi = (nfa + TILE - 1) / TILE;
+    const long long nt = tile_count(Rlo, Rhi);
+    const size_t need = (size_t)nt * 2 * TILE * NV * sizeof(double);
+    if (need > c.part_bytes) {
+        if (c.part) cudaFree(c.part);
+        c.part = nullptr;
+        c.part_bytes = 0;
+        if (cudaMalloc(&c.part, need) != cudaSuccess) return -3;
+        c.part_bytes = need;
+    }
+    const size_t smem = (size_t)8 * TILE * NV * sizeof(double);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_adjoint<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    k_adjoint<N><<<(unsigned)nt, 256, smem, c.stream>>>(c.sp, c.coef, c.Pd, c.bra, c.ket, c.detL, c.diagS, c.c, E,
+                                                        nfru, nfa, Rlo, c.part);
+    c.launches++;
+    const int nf = nfa - nfru;
+    k_adjoint_final<N><<<(nf * 32 + 255) / 256, 256, 0, c.stream>>>(c.part, c.params, nfru, nfa, Rlo, Rhi, c.grad);
+    c.launches++;
+    return last_err();
+}
+int launch_adjoint(Ctx& c, int nfru, int nfa, double E) { ECG_DISPATCH_N(c.n, adjoint_n, c, nfru, nfa, E) }
+
+int launch_plain_contract(Ctx& c, int nfo, int nfa, int nfru, double E)
+{
+    if (nfo <= 0) return 0;
+    k_contract<<<nfo, 256, 0, c.stream>>>(c.D, c.max_nfo, c.npt, c.c, E, nfo, nfa, nfru, c.grad);
+    c.launches++;
+    return last_err();
+}
+
+template <int N>
+static int batch_n(Ctx& c, int count, const double* pk, const double* pl, const int* term, int gradflag, cd* hs,
+                   cd* dk, cd* dl)
+{
+    if (count <= 0) return 0;
+    k_term_batch<N><<<(count + 127) / 128, 128, 0, c.stream>>>(c.sp, c.Pd, count, pk, pl, term, gradflag, hs, dk,
+                                                               dl);
+    c.launches++;
+    return last_err();
+}
+int launch_term_batch(Ctx& c, int count, const double* pk, const double* pl, const int* term, int gradflag, cd* hs,
+                      cd* dk, cd* dl)
+{
+    ECG_DISPATCH_N(c.n, batch_n, c, count, pk, pl, term, gradflag, hs, dk, dl)
+}
+
+}  // namespace ecg

@@ -1,0 +1,184 @@
+"""Host-side mirror of the reference's hot-path interface over the C ABI.
+
+Method names follow the Fortran routines they replace (ComputeMatElem,
+ComputeMatElemAndDeriv, GHEPIIS, EnergyIA/IAM, EnergyIB); indices are
+1-based and inclusive as in the Fortran.  GHEPIIS error codes 1 (zero
+pivot) and 2 (no convergence) are returned, as the reference returns them;
+negative ABI statuses (bad arguments, CUDA failures) raise EcgError.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import dptr, iptr
+
+__all__ = ["Context", "EcgError"]
+
+
+class EcgError(RuntimeError):
+    def __init__(self, status, what):
+        super().__init__(f"{what} failed with status {status}")
+        self.status = status
+
+
+def _check(status, what):
+    if status < 0:
+        raise EcgError(status, what)
+    return status
+
+
+class Context:
+    """One basis on one GPU: device copies of Glob_NonlinParam, Glob_H,
+    Glob_S, Glob_diagS, Glob_invD, Glob_c, Glob_LastEigvector, Glob_D."""
+
+    def __init__(self, system, ld, max_nfo=0, method="I", device=0):
+        self.lib = _lib.load()
+        self.system = system
+        self.ld = int(ld)
+        self.npt = system.npt
+        self.np = system.np
+        mm = np.ascontiguousarray(system.mass_matrix_cm, dtype=np.float64)
+        ch = np.ascontiguousarray(system.charges, dtype=np.float64)
+        ym = np.ascontiguousarray(system.yhy_mats_cm, dtype=np.int32)
+        yc = np.ascontiguousarray(system.yhy_coeffs, dtype=np.int32)
+        h = C.c_void_p()
+        _check(self.lib.ecg_ctx_create(system.n, dptr(mm), dptr(ch), system.T, iptr(ym), iptr(yc), self.ld,
+                                       int(max_nfo), method.encode(), int(device), C.byref(h)), "ecg_ctx_create")
+        self.h = h
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.ecg_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- data ---------------------------------------------------------------
+    def set_params(self, params, first=1):
+        """params: (count, npt) array of (vech L, vech B) rows."""
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        if p.ndim != 2 or p.shape[1] != self.npt:
+            raise ValueError(f"params must be (count, {self.npt})")
+        _check(self.lib.ecg_set_params(self.h, dptr(p), int(first), p.shape[0]), "ecg_set_params")
+
+    def matrices(self, n):
+        H = np.zeros((n, n), dtype=np.complex128, order="F")
+        S = np.zeros((n, n), dtype=np.complex128, order="F")
+        dS = np.zeros(n)
+        dH = np.zeros(n)
+        iD = np.zeros(n, dtype=np.complex128)
+        _check(self.lib.ecg_get_matrices(self.h, n, H.ctypes.data_as(_lib._dp), S.ctypes.data_as(_lib._dp), n,
+                                         dptr(dS), dptr(dH), iD.ctypes.data_as(_lib._dp)), "ecg_get_matrices")
+        return H, S, dS, dH, iD
+
+    def vectors(self, n):
+        c = np.zeros(n, dtype=np.complex128)
+        x = np.zeros(n, dtype=np.complex128)
+        _check(self.lib.ecg_get_vectors(self.h, n, c.ctypes.data_as(_lib._dp), x.ctypes.data_as(_lib._dp)),
+               "ecg_get_vectors")
+        return c, x
+
+    def set_vectors(self, n, c=None, last_eigvec=None):
+        cc = None if c is None else np.ascontiguousarray(c, dtype=np.complex128)
+        xx = None if last_eigvec is None else np.ascontiguousarray(last_eigvec, dtype=np.complex128)
+        _check(self.lib.ecg_set_vectors(self.h, n, None if cc is None else cc.ctypes.data_as(_lib._dp),
+                                        None if xx is None else xx.ctypes.data_as(_lib._dp)), "ecg_set_vectors")
+
+    def deriv(self, nfo, nfa):
+        D = np.zeros((nfa, nfo, 2 * self.npt), dtype=np.complex128)
+        _check(self.lib.ecg_get_deriv(self.h, nfo, nfa, D.ctypes.data_as(_lib._dp)), "ecg_get_deriv")
+        return np.transpose(D, (2, 1, 0))  # Glob_D(m, i, j)
+
+    def gradient(self, nfo):
+        g = np.zeros(nfo * self.npt)
+        _check(self.lib.ecg_get_gradient(self.h, nfo, dptr(g)), "ecg_get_gradient")
+        return g
+
+    # -- reference routines -------------------------------------------------
+    def compute_mat_elem(self, nmin, nmax, approx_energy):
+        """ComputeMatElem(Nmin, Nmax) with StoreHS, src/matform.f90:119-230."""
+        _check(self.lib.ecg_compute_mat_elem(self.h, nmin, nmax, float(approx_energy)), "ecg_compute_mat_elem")
+
+    def compute_mat_elem_and_deriv(self, nmin, nmax, nfru, approx_energy):
+        """ComputeMatElemAndDeriv(Nmin, Nmax) with StoreHSD, src/matform.f90:234-360."""
+        _check(self.lib.ecg_compute_mat_elem_and_deriv(self.h, nmin, nmax, nfru, float(approx_energy)),
+               "ecg_compute_mat_elem_and_deriv")
+
+    def ghepiis(self, k, n, apprlambda, tol, max_iter=20, specif_norm=-1):
+        """GHEPIIS, src/linalg.f90:1781-1926.  Returns (lambda, RelAcc,
+        NumIter, ErrorCode)."""
+        lam, ra, it = C.c_double(), C.c_double(), C.c_int()
+        err = _check(self.lib.ecg_ghepiis(self.h, k, n, float(apprlambda), float(tol), int(max_iter),
+                                          int(specif_norm), C.byref(lam), C.byref(ra), C.byref(it)), "ecg_ghepiis")
+        return lam.value, ra.value, it.value, err
+
+    def energy_ia(self, nmin, nmax, approx_energy, tol, max_iter=20, mat_elem_needed=True, specif_norm=-1):
+        """EnergyIA (specif_norm=-1) / EnergyIAM (0), src/workproc.f90:1954-2060.
+        Returns (E, ErrorCode, NumIter)."""
+        e, it = C.c_double(), C.c_int()
+        err = _check(self.lib.ecg_energy_ia(self.h, nmin, nmax, int(bool(mat_elem_needed)), float(approx_energy),
+                                            float(tol), int(max_iter), int(specif_norm), C.byref(e), C.byref(it)),
+                     "ecg_energy_ia")
+        return e.value, err, it.value
+
+    def _energy_ib(self, fn, name, nfru, nfa, approx_energy, tol, max_iter, mat_elem_needed, want_grad):
+        e, it = C.c_double(), C.c_int()
+        g = np.zeros((nfa - nfru) * self.npt) if want_grad else None
+        err = _check(fn(self.h, nfru, nfa, int(bool(mat_elem_needed)), float(approx_energy), float(tol),
+                        int(max_iter), C.byref(e), dptr(g), C.byref(it)), name)
+        return e.value, g, err, it.value
+
+    def energy_ib(self, nfru, nfa, approx_energy, tol, max_iter=20, mat_elem_needed=True, want_grad=True):
+        """EnergyIB, src/workproc.f90:2063-2154 (plain: Glob_D formed and
+        contracted).  Returns (E, gradient, ErrorCode, NumIter)."""
+        return self._energy_ib(self.lib.ecg_energy_ib, "ecg_energy_ib", nfru, nfa, approx_energy, tol, max_iter,
+                               mat_elem_needed, want_grad)
+
+    def energy_ib_adjoint(self, nfru, nfa, approx_energy, tol, max_iter=20, mat_elem_needed=True, want_grad=True):
+        """EnergyIB through the fused adjoint pass (no Glob_D)."""
+        return self._energy_ib(self.lib.ecg_energy_ib_adjoint, "ecg_energy_ib_adjoint", nfru, nfa, approx_energy,
+                               tol, max_iter, mat_elem_needed, want_grad)
+
+    def matrix_elements(self, pk, pl, terms, gradflag=0):
+        """MatrixElements for a batch: returns H, S (count,) and Dk, Dl
+        (count, 4np) complex (None when not requested)."""
+        pk = np.ascontiguousarray(pk, dtype=np.float64)
+        pl = np.ascontiguousarray(pl, dtype=np.float64)
+        t = np.ascontiguousarray(terms, dtype=np.int32)
+        cnt = t.size
+        hs = np.zeros((cnt, 2), dtype=np.complex128)
+        dk = np.zeros((cnt, 4 * self.np), dtype=np.complex128) if gradflag in (1, 3) else None
+        dl = np.zeros((cnt, 4 * self.np), dtype=np.complex128) if gradflag in (2, 3) else None
+        _check(self.lib.ecg_matrix_elements(self.h, cnt, dptr(pk), dptr(pl), iptr(t), int(gradflag),
+                                            hs.ctypes.data_as(_lib._dp),
+                                            None if dk is None else dk.ctypes.data_as(_lib._dp),
+                                            None if dl is None else dl.ctypes.data_as(_lib._dp)),
+               "ecg_matrix_elements")
+        return hs[:, 0], hs[:, 1], dk, dl
+
+    # -- diagnostics --------------------------------------------------------
+    def launch_count(self):
+        return int(self.lib.ecg_launch_count(self.h))
+
+    def set_timing(self, on=True):
+        _check(self.lib.ecg_set_timing(self.h, int(bool(on))), "ecg_set_timing")
+
+    def stage_ms(self):
+        ms = np.zeros(4)
+        _check(self.lib.ecg_get_stage_ms(self.h, dptr(ms)), "ecg_get_stage_ms")
+        return ms
+
+    def sync(self):
+        _check(self.lib.ecg_sync(self.h), "ecg_sync")

@@ -1,0 +1,130 @@
+/*
+ * ecg_abi.h -- C ABI of libecgb200.so, the B200 drop-in for the variational
+ * hot path of ATOM-MOL-nonBO (matrix elements over explicitly correlated
+ * complex Gaussians, H/S assembly, the inverse-iteration solve of HC = ESC
+ * and the gradient with respect to the nonlinear parameters).
+ *
+ * The reference's routines are Fortran module procedures that talk through
+ * module globals (src/globvars.f90).  Here the globals live in an opaque
+ * context, one per basis, whose device arrays mirror them:
+ *     Glob_NonlinParam (npt x K)   Glob_H, Glob_S (ld x ld)   Glob_diagS,
+ *     Glob_diagH   Glob_invD   Glob_c   Glob_LastEigvector   Glob_D.
+ * Conventions:
+ *   - every function returns an int status: 0 = success; 1 / 2 are the
+ *     GHEPIIS ErrorCodes (1 = exactly zero pivot, 2 = not converged);
+ *     negative values are ECG_E* below.  Nothing aborts the process.
+ *   - basis indices are 1-based and inclusive, as in the Fortran callers;
+ *     matrices are column-major; complex numbers are (re, im) double pairs
+ *     (Fortran complex(8), C double _Complex).
+ *   - pointers named *_host are host memory, copied during the call only.
+ *   - one context is used by one host thread; all work is ordered on the
+ *     context's CUDA stream.
+ */
+#ifndef ECG_ABI_H
+#define ECG_ABI_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ECG_OK 0
+#define ECG_ESINGULAR 1     /* GHEPIIS ErrorCode=1, src/linalg.f90:1862-1863 */
+#define ECG_ENOCONV 2       /* GHEPIIS ErrorCode=2, src/linalg.f90:1864-1869 */
+#define ECG_EARG (-1)       /* bad argument (size, index range, method) */
+#define ECG_ECUDA (-2)      /* CUDA runtime error */
+#define ECG_ENOMEM (-3)     /* device allocation failed */
+#define ECG_ENODEV (-4)     /* no CUDA device */
+
+typedef struct ecg_ctx ecg_ctx;
+
+/* Create a context for one system and basis capacity.
+ * Replaces the array allocation and ProgramDataInit outputs consumed by the
+ * hot path (src/workproc.f90:575-1202): n pseudo-particles (1..5),
+ * mass_matrix_host = Glob_MassMatrix (n x n), charges_host = (q0, q1..qn)
+ * = (Glob_PseudoCharge0, Glob_PseudoCharge), nterms Y^+Y terms with
+ * yhy_mats_host = Glob_YHYMatr (n x n x nterms, integer) and
+ * yhy_coeffs_host = Glob_YHYCoeff.  ld = Glob_HSLeadDim (max basis size),
+ * max_nfo = the second extent of Glob_D (0: no plain derivative storage),
+ * method = Glob_GSEPSolutionMethod ('I' or 'G').  device = CUDA ordinal. */
+int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_host, int nterms,
+                   const int* yhy_mats_host, const int* yhy_coeffs_host, int ld, int max_nfo, char method,
+                   int device, ecg_ctx** out);
+int ecg_ctx_destroy(ecg_ctx* ctx);
+
+/* Glob_NonlinParam(1:npt, first:first+count-1) = params_host (npt x count). */
+int ecg_set_params(ecg_ctx* ctx, const double* params_host, int first, int count);
+
+/* ComputeMatElem(Nmin,Nmax) + StoreHS, src/matform.f90:119-230 and :11-51.
+ * approx_energy = Glob_ApproxEnergy (lambda~).  Rows Nmin..Nmax of the
+ * lower triangle are computed; 'I' storage keeps H - lambda~ S in the lower
+ * triangle of H and the full Hermitian S; 'G' storage keeps the strict lower
+ * triangles of H and S plus diagS, diagH. */
+int ecg_compute_mat_elem(ecg_ctx* ctx, int nmin, int nmax, double approx_energy);
+
+/* ComputeMatElemAndDeriv(Nmin,Nmax) + StoreHSD, src/matform.f90:234-360 and
+ * :55-115: as above plus Glob_D(1:2npt, i-nfru, j).  Requires
+ * nfru < Nmin and Nmax - nfru <= max_nfo. */
+int ecg_compute_mat_elem_and_deriv(ecg_ctx* ctx, int nmin, int nmax, int nfru, double approx_energy);
+
+/* GHEPIIS(k,n,Glob_H,...,Glob_invD,Glob_S,...,apprlambda,Glob_c,w,Tol,
+ * lambda,Glob_LastEigvector,RelAcc,MaxIter,SpecifNorm,NumIter,ErrorCode),
+ * src/linalg.f90:1781-1926, on the context's device arrays: the LDL^H
+ * factor of rows 1..k-1 is reused, rows k..n are factorised; the start
+ * vector is Glob_c and the eigenvector lands in Glob_LastEigvector.
+ * Returns ErrorCode. */
+int ecg_ghepiis(ecg_ctx* ctx, int k, int n, double apprlambda, double tol, int max_iter, int specif_norm,
+                double* lambda, double* rel_acc, int* num_iter);
+
+/* EnergyIA / EnergyIAM, src/workproc.f90:1954-2060: optional
+ * ComputeMatElem(Nmin,Nmax), then Glob_c = Glob_LastEigvector and GHEPIIS
+ * with SpecifNorm -1 (IA) or 0 (IAM).  Returns ErrorCode. */
+int ecg_energy_ia(ecg_ctx* ctx, int nmin, int nmax, int mat_elem_needed, double approx_energy, double tol,
+                  int max_iter, int specif_norm, double* energy, int* num_iter);
+
+/* EnergyIB, src/workproc.f90:2063-2154 (plain drop-in): optional
+ * ComputeMatElemAndDeriv(nfru+1, nfa), GHEPIIS(nfru+1, nfa, ..., SpecifNorm
+ * 0), then the gradient contraction over Glob_D.  grad_host receives npt*nfo
+ * values ordered (vechL_i, vechB_i) for i = nfru+1..nfa; NULL leaves the
+ * gradient on the device (ecg_get_gradient). */
+int ecg_energy_ib(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, double approx_energy, double tol,
+                  int max_iter, double* energy, double* grad_host, int* num_iter);
+
+/* Same result as ecg_energy_ib from a fused adjoint pass: H, S without
+ * derivatives, GHEPIIS, then one pass over the pairs of rows nfru+1..nfa
+ * that recomputes each pair term and contracts its derivatives with
+ * c_k^* c_l on the fly; Glob_D is neither formed nor read. */
+int ecg_energy_ib_adjoint(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, double approx_energy, double tol,
+                          int max_iter, double* energy, double* grad_host, int* num_iter);
+
+/* Device -> host copies of the context arrays (any pointer may be NULL).
+ * H_host, S_host: n x n with leading dimension ld_host. */
+int ecg_get_matrices(ecg_ctx* ctx, int n, double* H_host, double* S_host, int ld_host, double* diagS_host,
+                     double* diagH_host, double* invD_host);
+int ecg_get_vectors(ecg_ctx* ctx, int n, double* c_host, double* last_eigvec_host);
+int ecg_set_vectors(ecg_ctx* ctx, int n, const double* c_host, const double* last_eigvec_host);
+int ecg_get_gradient(ecg_ctx* ctx, int nfo, double* grad_host);
+/* Glob_D(1:2npt, 1:nfo, 1:nfa) with leading extents (2npt, nfo). */
+int ecg_get_deriv(ecg_ctx* ctx, int nfo, int nfa, double* D_host);
+
+/* MatrixElements(Paramk, Paraml, P, Hkl, Skl, Dk, Dl, gradflag),
+ * src/matelem.f90:12-750, for count independent calls.  P is the context's
+ * Y^+Y matrix number term_host[i] (0-based).  hs_host receives (Hkl, Skl)
+ * per call (4 doubles); dk_host / dl_host receive 4np complex values per
+ * call when gradflag asks for them (may be NULL otherwise). */
+int ecg_matrix_elements(ecg_ctx* ctx, int count, const double* pk_host, const double* pl_host,
+                        const int* term_host, int gradflag, double* hs_host, double* dk_host, double* dl_host);
+
+/* Diagnostics: kernel launches issued by this context so far, and the
+ * device time (ms) of the stages of the last energy call:
+ * [0] pair pass(es) for H,S  [1] LDL^H  [2] inverse iterations
+ * [3] gradient (derivative pass + contraction, or adjoint pass). */
+long long ecg_launch_count(ecg_ctx* ctx);
+int ecg_set_timing(ecg_ctx* ctx, int on);
+int ecg_get_stage_ms(ecg_ctx* ctx, double* ms4);
+/* Block until all work queued on the context's stream has finished. */
+int ecg_sync(ecg_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ECG_ABI_H */

@@ -1,0 +1,158 @@
+"""ctypes front end of the CPU oracle (liboracle.so, built from
+ecg_oracle.c by the Makefile in this folder).
+
+TEST INFRASTRUCTURE ONLY: the parity checker and the timed CPU baseline.
+The product (libecgb200.so and the ecg_b200 package) never imports this.
+
+The glue functions below restate EnergyIA / EnergyIAM / EnergyIB
+(src/workproc.f90:1954-2154) on top of the C restatements of
+ComputeMatElem(AndDeriv), GHEPIIS and the gradient contraction.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_lib = None
+
+
+def build():
+    src = os.path.join(HERE, "ecg_oracle.c")
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def load():
+    global _lib
+    if _lib is None:
+        build()
+        lib = C.CDLL(LIB)
+        lib.orc_set_system.argtypes = [C.c_int, C.c_int, _dp, _dp, _ip, _ip]
+        lib.orc_set_system.restype = C.c_int
+        lib.orc_matrix_elements.argtypes = [_dp, _dp, _ip, _dp, _dp, _dp, C.c_int]
+        lib.orc_compute_mat_elem.argtypes = [_dp, C.c_int, C.c_int, C.c_char, C.c_double, _dp, _dp, C.c_int, _dp, _dp]
+        lib.orc_compute_mat_elem_and_deriv.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_char, C.c_double, _dp,
+                                                       _dp, C.c_int, _dp, _dp, _dp, C.c_int]
+        lib.orc_ldlhf.argtypes = [C.c_int, C.c_int, _dp, C.c_int, _dp, _dp]
+        lib.orc_ldlhf.restype = C.c_int
+        lib.orc_ldlhs.argtypes = [C.c_int, _dp, C.c_int, _dp, _dp, _dp]
+        lib.orc_vmmhmv.argtypes = [C.c_int, _dp, C.c_int, _dp]
+        lib.orc_vmmhmv.restype = C.c_double
+        lib.orc_ghepiis.argtypes = [C.c_int, C.c_int, _dp, C.c_int, _dp, _dp, C.c_int, C.c_double, _dp, _dp,
+                                    C.c_double, _dp, C.c_int, C.c_int, _dp, _ip]
+        lib.orc_ghepiis.restype = C.c_int
+        lib.orc_gradient_contract.argtypes = [C.c_int, C.c_int, C.c_int, _dp, C.c_int, _dp, C.c_double, _dp]
+        lib.orc_set_threads.argtypes = [C.c_int]
+        lib.orc_get_threads.restype = C.c_int
+        _lib = lib
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+def set_threads(n):
+    load().orc_set_threads(int(n))
+
+
+def get_threads():
+    return load().orc_get_threads()
+
+
+class Oracle:
+    """Oracle state for one system (mirrors the Glob_* arrays on the host)."""
+
+    def __init__(self, system, ld, max_nfo=0):
+        self.lib = load()
+        self.sys = system
+        self.n, self.np, self.npt = system.n, system.np, system.npt
+        self.ld = ld
+        mm = np.ascontiguousarray(system.mass_matrix_cm, dtype=np.float64)
+        ch = np.ascontiguousarray(system.charges, dtype=np.float64)
+        ym = np.ascontiguousarray(system.yhy_mats_cm, dtype=np.int32)
+        yc = np.ascontiguousarray(system.yhy_coeffs, dtype=np.int32)
+        self._keep = (mm, ch, ym, yc)
+        assert self.lib.orc_set_system(self.n, system.T, _p(mm), _p(ch), ym.ctypes.data_as(_ip),
+                                       yc.ctypes.data_as(_ip)) == 0
+        self.H = np.zeros((ld, ld), dtype=np.complex128, order="F")
+        self.S = np.zeros((ld, ld), dtype=np.complex128, order="F")
+        self.diagS = np.zeros(ld)
+        self.diagH = np.zeros(ld)
+        self.invD = np.zeros(ld, dtype=np.complex128)
+        self.c = np.zeros(ld, dtype=np.complex128)
+        self.last = np.zeros(ld, dtype=np.complex128)
+        self.max_nfo = max_nfo
+        self.D = np.zeros((2 * self.npt, max(max_nfo, 1), ld), dtype=np.complex128, order="F") if max_nfo else None
+        self.params = None
+
+    def activate(self):
+        """Re-install this system in the C globals (one system at a time)."""
+        mm, ch, ym, yc = self._keep
+        self.lib.orc_set_system(self.n, self.sys.T, _p(mm), _p(ch), ym.ctypes.data_as(_ip), yc.ctypes.data_as(_ip))
+
+    def set_params(self, params):
+        self.params = np.ascontiguousarray(params, dtype=np.float64)
+
+    # MatrixElements with an explicit permutation matrix
+    def matrix_elements(self, pk, pl, P, gradflag=0):
+        pk = np.ascontiguousarray(pk, dtype=np.float64)
+        pl = np.ascontiguousarray(pl, dtype=np.float64)
+        Pcm = np.ascontiguousarray(np.asarray(P, dtype=np.int32).T).ravel()
+        hs = np.zeros(2, dtype=np.complex128)
+        dk = np.zeros(4 * self.np, dtype=np.complex128)
+        dl = np.zeros(4 * self.np, dtype=np.complex128)
+        self.lib.orc_matrix_elements(_p(pk), _p(pl), Pcm.ctypes.data_as(_ip), _p(hs), _p(dk), _p(dl), gradflag)
+        return hs[0], hs[1], dk, dl
+
+    def compute_mat_elem(self, nmin, nmax, approx_e, method="I"):
+        self.lib.orc_compute_mat_elem(_p(self.params), nmin, nmax, method.encode(), approx_e, _p(self.H), _p(self.S),
+                                      self.ld, _p(self.diagS), _p(self.diagH))
+
+    def compute_mat_elem_and_deriv(self, nmin, nmax, nfru, approx_e, method="I"):
+        self.lib.orc_compute_mat_elem_and_deriv(_p(self.params), nmin, nmax, nfru, method.encode(), approx_e,
+                                                _p(self.H), _p(self.S), self.ld, _p(self.diagS), _p(self.diagH),
+                                                _p(self.D), self.D.shape[1])
+
+    def ghepiis(self, k, n, apprlambda, tol, max_iter=20, specif_norm=-1):
+        """GHEPIIS on (H, invD, S) with start vector c; eigenvector -> last.
+        Returns (lambda, RelAcc, NumIter, ErrorCode)."""
+        w = np.zeros(self.ld, dtype=np.complex128)
+        out = np.zeros(2)
+        it = np.zeros(1, dtype=np.int32)
+        err = self.lib.orc_ghepiis(k, n, _p(self.H), self.ld, _p(self.invD), _p(self.S), self.ld, apprlambda,
+                                   _p(self.c), _p(w), tol, _p(self.last), max_iter, specif_norm, _p(out),
+                                   it.ctypes.data_as(_ip))
+        return out[0], out[1], int(it[0]), err
+
+    # EnergyIA / EnergyIAM, src/workproc.f90:1954-2060
+    def energy_ia(self, nmin, nmax, approx_e, tol, max_iter=20, mat_elem_needed=True, specif_norm=-1):
+        if mat_elem_needed:
+            self.compute_mat_elem(nmin, nmax, approx_e)
+        if nmax == 1:
+            return self.H[0, 0].real + approx_e, 0, 1
+        self.c[:nmax] = self.last[:nmax]
+        lam, ra, it, err = self.ghepiis(nmin, nmax, approx_e, tol, max_iter, specif_norm)
+        return lam, err, it
+
+    # EnergyIB, src/workproc.f90:2063-2154
+    def energy_ib(self, nfru, nfa, approx_e, tol, max_iter=20, mat_elem_needed=True):
+        nfo = nfa - nfru
+        if mat_elem_needed:
+            self.compute_mat_elem_and_deriv(nfru + 1, nfa, nfru, approx_e)
+        if nfa == 1:
+            E, err, it = self.H[0, 0].real + approx_e, 0, 1
+            self.c[0] = 1.0
+        else:
+            self.c[:nfa] = self.last[:nfa]
+            E, ra, it, err = self.ghepiis(nfru + 1, nfa, approx_e, tol, max_iter, 0)
+            self.c[:nfa] = self.last[:nfa]
+        g = np.zeros(nfo * self.npt)
+        self.lib.orc_gradient_contract(nfo, nfa, nfru, _p(self.D), self.D.shape[1], _p(self.c), E, _p(g))
+        return E, g, err, it
