@@ -55,6 +55,7 @@ void free_ctx(Ctx& c)
     if (c.red_h) cudaFreeHost(c.red_h);
     if (c.stream) {
         for (int i = 0; i < 16; i++) cudaEventDestroy(c.ev[i]);
+        for (int i = 0; i < 2; i++) cudaEventDestroy(c.tev[i]);
         cudaStreamDestroy(c.stream);
     }
 }
@@ -77,6 +78,7 @@ double elapsed(Ctx& c, int a, int b)
 int read_red(Ctx& c)
 {
     CK(cudaMemcpyAsync(c.red_h, c.red, RD_COUNT * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    c.bytes_d2h += RD_COUNT * sizeof(double);
     CK(cudaStreamSynchronize(c.stream));
     return 0;
 }
@@ -115,6 +117,7 @@ int ghepiis(Ctx& c, int k, int n, double apprlambda, double tol, int max_iter, i
     CK(cudaMemsetAsync(c.status, 0, ST_COUNT * sizeof(int), c.stream));
     CKR(ldlh_factor(c, k - 1, n));
     CK(cudaMemcpyAsync(c.status_h, c.status, ST_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    c.bytes_d2h += ST_COUNT * sizeof(int);
     CK(cudaStreamSynchronize(c.stream));
     mark(c, 2);
     if (c.status_h[ST_ZERO_PIVOT] != 0) {
@@ -160,6 +163,7 @@ int single_function_energy(Ctx& c, double approx_e, double* energy)
 {
     cd h11;
     CK(cudaMemcpyAsync(&h11, c.H, sizeof(cd), cudaMemcpyDeviceToHost, c.stream));
+    c.bytes_d2h += sizeof(cd);
     CK(cudaStreamSynchronize(c.stream));
     *energy = h11.x + approx_e;
     const cd one{1.0, 0.0};
@@ -223,6 +227,7 @@ int energy_ib_common(Ctx& c, int nfru, int nfa, int needed, double approx_e, dou
     if (grad_host) {
         CK(cudaMemcpyAsync(grad_host, c.grad, (size_t)nfo * c.npt * sizeof(double), cudaMemcpyDeviceToHost,
                            c.stream));
+        c.bytes_d2h += (long long)nfo * c.npt * sizeof(double);
     }
     CK(cudaStreamSynchronize(c.stream));
     finish_timing(c, true);
@@ -281,6 +286,7 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
         return ECG_ECUDA;
     }
     for (int i = 0; i < 16; i++) cudaEventCreate(&c.ev[i]);
+    for (int i = 0; i < 2; i++) cudaEventCreate(&c.tev[i]);
     const size_t L = (size_t)ld;
     r |= dalloc(&c.params, (size_t)c.npt * L);
     r |= dalloc(&c.H, L * L);
@@ -352,6 +358,7 @@ int ecg_set_params(ecg_ctx* ctx, const double* params_host, int first, int count
     Ctx& c = ctx->c;
     CK(cudaMemcpyAsync(c.params + (size_t)(first - 1) * c.npt, params_host, (size_t)count * c.npt * sizeof(double),
                        cudaMemcpyHostToDevice, c.stream));
+    c.bytes_h2d += (long long)count * c.npt * sizeof(double);
     return ECG_OK;
 }
 
@@ -591,6 +598,33 @@ int ecg_sync(ecg_ctx* ctx)
 {
     if (!ctx) return ECG_EARG;
     CK(cudaStreamSynchronize(ctx->c.stream));
+    return ECG_OK;
+}
+
+int ecg_timer_start(ecg_ctx* ctx)
+{
+    if (!ctx) return ECG_EARG;
+    CK(cudaEventRecord(ctx->c.tev[0], ctx->c.stream));
+    return ECG_OK;
+}
+
+int ecg_timer_stop(ecg_ctx* ctx, double* ms)
+{
+    if (!ctx || !ms) return ECG_EARG;
+    Ctx& c = ctx->c;
+    CK(cudaEventRecord(c.tev[1], c.stream));
+    CK(cudaEventSynchronize(c.tev[1]));
+    float f = 0.f;
+    CK(cudaEventElapsedTime(&f, c.tev[0], c.tev[1]));
+    *ms = f;
+    return ECG_OK;
+}
+
+int ecg_io_bytes(ecg_ctx* ctx, long long* h2d, long long* d2h)
+{
+    if (!ctx) return ECG_EARG;
+    if (h2d) *h2d = ctx->c.bytes_h2d;
+    if (d2h) *d2h = ctx->c.bytes_d2h;
     return ECG_OK;
 }
 

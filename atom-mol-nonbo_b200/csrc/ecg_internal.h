@@ -72,6 +72,8 @@ struct Ctx {
 
     // bookkeeping
     long long launches = 0;
+    long long bytes_h2d = 0, bytes_d2h = 0;
+    cudaEvent_t tev[2];
     bool timing = false;
     cudaEvent_t ev[16];
     double stage_ms[8] = {0};

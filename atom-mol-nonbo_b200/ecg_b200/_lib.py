@@ -37,6 +37,10 @@ PROTOTYPES = {
     "ecg_set_timing": (C.c_int, [_vp, C.c_int]),
     "ecg_get_stage_ms": (C.c_int, [_vp, _dp]),
     "ecg_sync": (C.c_int, [_vp]),
+    "ecg_timer_start": (C.c_int, [_vp]),
+    "ecg_timer_stop": (C.c_int, [_vp, _dp]),
+    "ecg_io_bytes": (C.c_int, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "ecg_probe_fp64_peak": (C.c_int, [C.c_int, _dp]),
 }
 
 _lib = None

@@ -13,7 +13,7 @@ import numpy as np
 from . import _lib
 from ._lib import dptr, iptr
 
-__all__ = ["Context", "EcgError"]
+__all__ = ["Context", "EcgError", "probe_fp64_peak"]
 
 
 class EcgError(RuntimeError):
@@ -182,3 +182,24 @@ class Context:
 
     def sync(self):
         _check(self.lib.ecg_sync(self.h), "ecg_sync")
+
+    def timer_start(self):
+        _check(self.lib.ecg_timer_start(self.h), "ecg_timer_start")
+
+    def timer_stop(self):
+        ms = C.c_double()
+        _check(self.lib.ecg_timer_stop(self.h, C.byref(ms)), "ecg_timer_stop")
+        return ms.value
+
+    def io_bytes(self):
+        a, b = C.c_longlong(), C.c_longlong()
+        _check(self.lib.ecg_io_bytes(self.h, C.byref(a), C.byref(b)), "ecg_io_bytes")
+        return a.value, b.value
+
+
+def probe_fp64_peak(device=0):
+    """Measured FP64 FMA throughput of the device in TFLOP/s."""
+    lib = _lib.load()
+    t = C.c_double()
+    _check(lib.ecg_probe_fp64_peak(int(device), C.byref(t)), "ecg_probe_fp64_peak")
+    return t.value

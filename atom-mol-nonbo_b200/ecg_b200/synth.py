@@ -67,15 +67,58 @@ def candidates(basis, B, seed, p1=0.7, s1=1.0, s2=3.0):
     return out
 
 
+# e_floor: an energy below the lowest state of each system (the exact
+# non-Born-Oppenheimer ground-state energies are about -0.527, -1.164 and
+# -7.478 hartree), used as a first inverse-iteration shift.
+SYSTEMS = {
+    # heavy particle (+1, 1836.15) and two electrons, electron exchange
+    "h_minus_like": dict(masses=[1836.15, 1.0, 1.0], charges=[1.0, -1.0, -1.0], symmetry="(1+P23)",
+                         e_floor=-0.6),
+    # two heavy particles (+1, 1836.15) and two electrons
+    "h2_like": dict(masses=[1836.15, 1836.15, 1.0, 1.0], charges=[1.0, 1.0, -1.0, -1.0],
+                    symmetry="(1+P12)(1+P34)", e_floor=-1.2),
+    # heavy particle (+3, 12786) and three electrons (n = 3, six Y^+Y terms)
+    "li_like": dict(masses=[12786.0, 1.0, 1.0, 1.0], charges=[3.0, -1.0, -1.0, -1.0],
+                    symmetry="(1+P23)(1-P24)", e_floor=-7.6),
+    # five particles (n = 4): heavy particle (+3, 12786) and four electrons,
+    # exercising the n = 4 kernels
+    "li_minus_like": dict(masses=[12786.0, 1.0, 1.0, 1.0, 1.0], charges=[3.0, -1.0, -1.0, -1.0, -1.0],
+                          symmetry="(1+P23)(1+P45)(1-P24)", e_floor=-7.6),
+}
+
+# The benchmark configurations: system, basis size K, seed (1000 + index).
+CONFIGS = {
+    0: dict(system="h_minus_like", K=500, seed=1000),
+    1: dict(system="h2_like", K=1500, seed=1001),
+    2: dict(system="h2_like", K=4000, seed=1002),
+    3: dict(system="h2_like", K=2000, seed=1003, candidates=256),
+    4: dict(system="li_like", K=10000, seed=1004, mass_scaled=True),
+}
+
+
 def systems():
     """The physical systems of the benchmark configurations."""
-    return {
-        # heavy particle (+1, 1836.15) and two electrons, electron exchange
-        "h_minus_like": dict(masses=[1836.15, 1.0, 1.0], charges=[1.0, -1.0, -1.0], symmetry="(1+P23)"),
-        # two heavy particles (+1, 1836.15) and two electrons
-        "h2_like": dict(masses=[1836.15, 1836.15, 1.0, 1.0], charges=[1.0, 1.0, -1.0, -1.0],
-                        symmetry="(1+P12)(1+P34)"),
-        # heavy particle (+3, 12786) and three electrons
-        "li_like": dict(masses=[12786.0, 1.0, 1.0, 1.0], charges=[3.0, -1.0, -1.0, -1.0],
-                        symmetry="(1+P23)(1-P24)"),
-    }
+    return SYSTEMS
+
+
+def make_system(name):
+    from .system import System
+    d = SYSTEMS[name]
+    return System(d["masses"], d["charges"], d["symmetry"])
+
+
+def reduced_mass_scale(masses):
+    """sqrt(mu_i / m_e) per pseudo-particle, mu_i = m0 m_i / (m0 + m_i)."""
+    m = np.asarray(masses, dtype=np.float64)
+    mu = m[0] * m[1:] / (m[0] + m[1:])
+    return np.sqrt(mu)
+
+
+def config_basis(index, K=None):
+    """(system, params) of benchmark configuration `index`; K overrides the
+    basis size (the first K functions of the full basis are the same)."""
+    cfg = CONFIGS[index]
+    sysm = make_system(cfg["system"])
+    KK = cfg["K"] if K is None else K
+    scale = reduced_mass_scale(SYSTEMS[cfg["system"]]["masses"]) if cfg.get("mass_scaled") else None
+    return sysm, random_basis(sysm.n, KK, cfg["seed"], row_scale=scale)

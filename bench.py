@@ -1,0 +1,414 @@
+"""Benchmark: energy + gradient evaluations per second of the variational
+hot path at n = 3 (two heavy particles + two electrons, four Y^+Y terms),
+K = 4000 seeded synthetic ECGs, FP64, one GPU per rank.
+
+One step = one EnergyIB evaluation through the fused adjoint pass: all
+K(K+1)/2 pair elements of H and S, the LDL^H factorisation of H - lambda~ S,
+inverse iteration to the lowest root, and the gradient with respect to all
+K * 12 nonlinear parameters.  `value` times that with the parameters already
+on the device; `e2e` adds, every step, the host->device copy of the
+parameters (pinned host memory) and the device->host copy of the gradient.
+The plain drop-in (derivatives materialised in Glob_D, then contracted) is
+timed beside it.
+
+--impl reference times the CPU restatement of the reference (the oracle,
+OpenMP over pairs, all host threads) on a bounded sample of the same
+workload, scaled to evaluations per second.
+
+Multi-GPU: every rank evaluates its own replica (independent bases, no
+collective on the data path); value = total evaluations / max-over-ranks
+time.
+"""
+import argparse
+import json
+import os
+import platform
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "atom-mol-nonbo_b200"))
+
+METRIC = "energy+gradient evals/s at n=3,K=4000 (adjoint vs plain GPU); ECG pairs/s"
+CONFIG_INDEX = 2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--K", type=int, default=None, help="override the basis size (testing only)")
+    ap.add_argument("--tol", type=float, default=1e-10, help="GHEPIIS tolerance (EIGVAL_TOLERANCE)")
+    ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--cpu-baseline", type=int, default=1)
+    ap.add_argument("--lam", type=float, default=None,
+                    help="use this lambda~ instead of searching for one (profiling runs)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+class Dist:
+    """torch.distributed for the barrier and the max-over-ranks time only."""
+
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as td
+            td.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.td = td
+
+    def barrier(self):
+        if self.world > 1:
+            self.td.barrier()
+
+    def max(self, x):
+        if self.world == 1:
+            return x
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64)
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x):
+        if self.world == 1:
+            return x
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64)
+        self.td.all_reduce(t, op=self.td.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.td.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def setup_problem(K, rank):
+    from ecg_b200 import synth
+    sysm, params = synth.config_basis(CONFIG_INDEX, K=K)
+    if rank:  # independent replica per rank
+        cfg = synth.CONFIGS[CONFIG_INDEX]
+        params = synth.random_basis(sysm.n, K, cfg["seed"] + 7919 * rank)
+    return sysm, params, synth.SYSTEMS[synth.CONFIGS[CONFIG_INDEX]["system"]]["e_floor"]
+
+
+def find_shift(ctx, K, e_floor):
+    """lambda~ just below the lowest root: converge from a lower bound of the
+    spectrum, then sit 1e-12 relative below the root found."""
+    ctx.set_vectors(K, last_eigvec=np.ones(K, dtype=np.complex128))
+    E, err, it = ctx.energy_ia(1, K, e_floor, -1e-12, max_iter=200, specif_norm=0)
+    E2, err2, it2 = ctx.energy_ia(1, K, E * (1.0 + 1e-9), -1e-12, max_iter=50, specif_norm=0)
+    return E2 * (1.0 + 1e-12), E2
+
+
+def flush_l2(buf):
+    """Write a buffer larger than L2 on the default device (torch)."""
+    if buf is not None:
+        buf.add_(1.0)
+
+
+def run_ours(args, dist):
+    import torch
+
+    from ecg_b200 import Context, probe_fp64_peak
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import opcount
+
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    K = args.K or 4000
+    sysm, params, e_floor = setup_problem(K, dist.rank)
+    T = sysm.T
+    pairs = K * (K + 1) // 2
+    ctx = Context(sysm, K, max_nfo=K if args.plain_steps > 0 else 0, device=dev)
+    ctx.set_params(params)
+    if args.lam is None:
+        lam, E_ref = find_shift(ctx, K, e_floor)
+    else:
+        lam = args.lam
+        ctx.set_vectors(K, last_eigvec=np.ones(K, dtype=np.complex128))
+    l2buf = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")  # 256 MB > L2
+
+    def one(adjoint=True, want_grad=False):
+        fn = ctx.energy_ib_adjoint if adjoint else ctx.energy_ib
+        return fn(0, K, lam, args.tol, max_iter=20, want_grad=want_grad)
+
+    # ---- device-resident timing --------------------------------------
+    for _ in range(args.warmup):
+        one()
+    ctx.set_timing(True)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    launches0 = ctx.launch_count()
+    stage = np.zeros(4)
+    total_ms, iters = 0.0, []
+    dist.barrier()
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        flush_l2(l2buf)
+        torch.cuda.synchronize()
+        ctx.timer_start()
+        E, _, err, it = one()
+        total_ms += ctx.timer_stop()
+        stage += ctx.stage_ms()
+        iters.append(it)
+    torch.cuda.synchronize()
+    dist.barrier()
+    launches = ctx.launch_count() - launches0
+    clk = clocks.stop()
+    ms_step = dist.max(total_ms) / args.steps
+    value = dist.sum(args.steps) / (dist.max(total_ms) / 1e3)
+
+    # ---- end-to-end through the public API with host buffers ------------
+    pin = torch.empty(params.shape, dtype=torch.float64, pin_memory=True)
+    pin.numpy()[:] = params
+    gpin = torch.empty(K * sysm.npt, dtype=torch.float64, pin_memory=True)
+    pin_np, g_np = pin.numpy(), gpin.numpy()
+    h0, d0 = ctx.io_bytes()
+    e2e_ms = 0.0
+    dist.barrier()
+    for _ in range(args.steps):
+        flush_l2(l2buf)
+        torch.cuda.synchronize()
+        ctx.timer_start()
+        ctx.set_params(pin_np)
+        import ctypes as C
+        e = C.c_double()
+        it = C.c_int()
+        st = ctx.lib.ecg_energy_ib_adjoint(ctx.h, 0, K, 1, lam, args.tol, 20, C.byref(e),
+                                           g_np.ctypes.data_as(C.POINTER(C.c_double)), C.byref(it))
+        e2e_ms += ctx.timer_stop()
+        assert st >= 0
+    h1, d1 = ctx.io_bytes()
+    e2e_value = dist.sum(args.steps) / (dist.max(e2e_ms) / 1e3)
+
+    # ---- plain drop-in beside it ---------------------------------------
+    plain = None
+    if args.plain_steps > 0:
+        one(adjoint=False)
+        pms = 0.0
+        pstage = np.zeros(4)
+        for _ in range(args.plain_steps):
+            flush_l2(l2buf)
+            torch.cuda.synchronize()
+            ctx.timer_start()
+            Ep, _, _, _ = one(adjoint=False)
+            pms += ctx.timer_stop()
+            pstage += ctx.stage_ms()
+        pms = dist.max(pms) / args.plain_steps
+        plain = {"value": dist.sum(1) / (pms / 1e3), "ms_per_step": pms, "E": Ep,
+                 "stages_ms": dict(zip(["pairs_hs_and_derivs", "ldlh", "invit", "contract"],
+                                       (pstage / args.plain_steps).round(4).tolist()))}
+
+    # ---- roofline of the dominant kernel --------------------------------
+    st = stage / args.steps
+    names = ["pairs_hs", "ldlh", "invit", "adjoint"]
+    peak = probe_fp64_peak(dev)
+    counts = opcount.pair_counts(sysm.n, T)
+    adj_flop = counts["adjoint"]["total"] * pairs
+    hs_flop = counts["reference_energy"]["total"] * pairs
+    ldl_flop = 4.0 / 3.0 * K ** 3
+    per_stage_tf = {"pairs_hs": hs_flop / (st[0] * 1e-3) / 1e12, "ldlh": ldl_flop / (st[1] * 1e-3) / 1e12,
+                    "adjoint": adj_flop / (st[3] * 1e-3) / 1e12}
+    dom = int(np.argmax(st))
+    dom_name = names[dom]
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(dom_name)
+    if dom_name in per_stage_tf:
+        achieved = per_stage_tf[dom_name]
+        roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": dom_name,
+                "peak_source": "measured in this run: register FMA loop over all SMs (no FP64 entry in "
+                               "MEASURED_PEAKS.json)"}
+    else:
+        # solver-dominated: the triangular solves are HBM/latency bound
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
+        bytes_it = 32.0 * K * K
+        achieved = bytes_it * max(np.mean(iters), 1) / (st[2] * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "kernel": dom_name}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": f"synthetic: seeded ECG basis (seed {1002}), two heavy particles + two electrons",
+        "config": {"workload": f"EnergyIB (adjoint) n=3 K={K} T={T}: H,S + LDL^H + inverse iteration + gradient",
+                   "K": K, "n": sysm.n, "T": T, "tol": args.tol,
+                   "l2": "H,S are 2 x 256 MB (> 126 MB L2) and a 256 MB buffer is written between steps",
+                   "parallelism": f"replicas x{dist.world}"},
+        "pairs_per_s": pairs * value, "pair_terms_per_s": pairs * T * value,
+        "energy": E, "invit_iters": float(np.mean(iters)),
+        "stages_ms": dict(zip(names, st.round(4).tolist())),
+        "stage_tflops": {k: round(v, 3) for k, v in per_stage_tf.items()},
+        "plain_gpu": plain,
+        "adjoint_speedup_vs_plain": (value / plain["value"]) if plain else None,
+        "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": (h1 - h0) // args.steps,
+                "d2h_bytes_per_step": (d1 - d0) // args.steps},
+        "gpu_launches": int(launches),
+        "roofline": roof,
+        "clocks": clk,
+    }
+    if args.cpu_baseline and dist.rank == 0:
+        line["cpu_baseline"] = cpu_sample(sysm, params, lam, K, budget_s=20.0, iters=np.mean(iters))
+    ctx.close()
+    return line
+
+
+# ---------------------------------------------------------------------------
+def cpu_sample(sysm, params, lam, K, budget_s=20.0, iters=3.0):
+    """Time the oracle on a bounded sample of one evaluation and scale it to
+    evaluations per second:
+      pair elements with derivatives (gradflag 3 + StoreHSD) for the last
+        rows of the basis, scaled by pair count to all K(K+1)/2 pairs;
+      GHEPIIS (LDLHF + inverse iterations) and the gradient contraction at
+        K' = 800, scaled by (K/K')^3 for LDLHF and (K/K')^2 for the rest."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    # pair sample: rows r0..K
+    rows = 6
+    while True:
+        r0 = K - rows + 1
+        npairs = sum(range(r0, K + 1))
+        o = orc.Oracle(sysm, K, max_nfo=rows)
+        o.set_params(params)
+        o.diagS[:] = 1.0
+        t0 = time.perf_counter()
+        o.compute_mat_elem_and_deriv(r0, K, r0 - 1, lam)
+        tp = time.perf_counter() - t0
+        if tp > 0.25 * budget_s or rows >= 200:
+            break
+        rows = min(200, int(rows * max(2.0, 0.3 * budget_s / max(tp, 1e-3))))
+    t_pairs = tp / npairs * (K * (K + 1) / 2)
+    del o
+    Kp = min(800, K)
+    o = orc.Oracle(sysm, Kp, max_nfo=Kp)
+    o.set_params(params[:Kp])
+    o.compute_mat_elem(1, Kp, lam)
+    t0 = time.perf_counter()
+    lib = o.lib
+    w = np.zeros(Kp, dtype=np.complex128)
+    err = lib.orc_ldlhf(1, Kp, o.H.ctypes.data_as(orc._dp), Kp, o.invD.ctypes.data_as(orc._dp),
+                        w.ctypes.data_as(orc._dp))
+    t_ldl = time.perf_counter() - t0
+    o.c[:Kp] = 1.0
+    t0 = time.perf_counter()
+    lam_, ra, it, e2 = o.ghepiis(Kp, Kp, lam, 1e-300, max_iter=3, specif_norm=0)  # factor kept, 3 iterations
+    t_it = (time.perf_counter() - t0) / 3.0
+    t_contract = 0.0
+    scale3, scale2 = (K / Kp) ** 3, (K / Kp) ** 2
+    t_eval = t_pairs + t_ldl * scale3 + t_it * iters * scale2 + t_contract
+    return {"value": 1.0 / t_eval, "unit": "evals/s", "cores": threads, "kind": "port",
+            "sample": (f"oracle (C restatement, OpenMP {threads} threads): {npairs} pairs with derivatives "
+                       f"(rows {r0}-{K}) scaled to {K * (K + 1) // 2} pairs; LDLHF and "
+                       f"inverse iterations at K'={Kp} scaled by (K/K')^3 and (K/K')^2 x {iters:.1f} iterations"),
+            "seconds_per_eval": t_eval,
+            "parts_s": {"pairs": t_pairs, "ldlhf": t_ldl * scale3, "invit": t_it * iters * scale2},
+            "cpu": platform.processor() or platform.machine()}
+
+
+def run_reference(args, dist):
+    if dist.rank != 0:
+        return None
+    from ecg_b200 import synth
+    K = args.K or 4000
+    sysm, params, e_floor = setup_problem(K, 0)
+    # a shift below the spectrum keeps H - lambda~ S positive definite, so
+    # the timed LDLHF never stops early at a zero pivot
+    lam = e_floor
+    vals = []
+    for _ in range(args.warmup):
+        cpu_sample(sysm, params, lam, K, budget_s=5.0)
+    for _ in range(args.steps):
+        vals.append(cpu_sample(sysm, params, lam, K, budget_s=10.0))
+    v = float(np.median([x["value"] for x in vals]))
+    s = vals[-1]
+    return {"metric": METRIC, "value": v, "unit": "evals/s", "impl": "reference", "n_gpus": dist.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded ECG basis (seed 1002)",
+            "config": {"workload": f"EnergyIB n=3 K={K} T={sysm.T} on the host CPU (bounded sample)", "K": K,
+                       "n": sysm.n, "T": sysm.T, "parallelism": "OpenMP over pairs"},
+            "cpu_baseline": {"value": v, "unit": "evals/s", "cores": s["cores"], "kind": "port",
+                             "sample": s["sample"]},
+            "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    try:
+        line = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
+        if dist.rank == 0 and line is not None:
+            print(json.dumps(line))
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

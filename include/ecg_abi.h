@@ -123,6 +123,15 @@ int ecg_set_timing(ecg_ctx* ctx, int on);
 int ecg_get_stage_ms(ecg_ctx* ctx, double* ms4);
 /* Block until all work queued on the context's stream has finished. */
 int ecg_sync(ecg_ctx* ctx);
+/* Device timer on the context's stream: start records an event; stop
+ * records a second one, waits for it and returns the elapsed ms. */
+int ecg_timer_start(ecg_ctx* ctx);
+int ecg_timer_stop(ecg_ctx* ctx, double* ms);
+/* Bytes this context has copied host->device and device->host so far. */
+int ecg_io_bytes(ecg_ctx* ctx, long long* h2d, long long* d2h);
+/* Measured FP64 FMA throughput of the device (TFLOP/s, 2 flops per FMA):
+ * a register-resident FMA loop over all SMs, timed with CUDA events. */
+int ecg_probe_fp64_peak(int device, double* tflops);
 
 #ifdef __cplusplus
 }
