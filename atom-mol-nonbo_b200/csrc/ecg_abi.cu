@@ -48,7 +48,7 @@ void free_ctx(Ctx& c)
 {
     void* ptrs[] = {c.params, c.H, c.S, c.diagS, c.diagH, c.invD, c.c, c.x, c.w, c.D, c.grad, c.Pd, c.coef,
                     c.bra, c.ket, c.detL, c.part, c.dw, c.linv, c.vbuf, c.status, c.red, c.counters, c.yv,
-                    c.zv, c.spart, c.colval};
+                    c.zv, c.spart, c.colval, c.dblk, c.flags};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c.status_h) cudaFreeHost(c.status_h);
@@ -78,8 +78,11 @@ double elapsed(Ctx& c, int a, int b)
 int read_red(Ctx& c)
 {
     CK(cudaMemcpyAsync(c.red_h, c.red, RD_COUNT * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-    c.bytes_d2h += RD_COUNT * sizeof(double);
+    CK(cudaMemcpyAsync(c.status_h, c.status, ST_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    c.bytes_d2h += RD_COUNT * sizeof(double) + ST_COUNT * sizeof(int);
     CK(cudaStreamSynchronize(c.stream));
+    // a cooperative solve that gave up waiting leaves an unusable step
+    if (c.status_h[ST_SOLVE_TIMEOUT]) return ECG_ECUDA;
     return 0;
 }
 
@@ -313,6 +316,8 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
     r |= dalloc(&c.counters, (size_t)4);
     r |= dalloc(&c.spart, (size_t)SOLVE_G_MAX * LDL_NB);
     r |= dalloc(&c.colval, 2 * L);
+    r |= dalloc(&c.dblk, L + 2);
+    r |= dalloc(&c.flags, L + 2);
     if (!r) {
         if (cudaMallocHost((void**)&c.status_h, ST_COUNT * sizeof(int)) != cudaSuccess ||
             cudaMallocHost((void**)&c.red_h, RD_COUNT * sizeof(double)) != cudaSuccess) {
@@ -330,6 +335,7 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
               cudaMemset(c.H, 0, L * L * sizeof(cd)) == cudaSuccess &&
               cudaMemset(c.S, 0, L * L * sizeof(cd)) == cudaSuccess &&
               cudaMemset(c.counters, 0, 4 * sizeof(int)) == cudaSuccess &&
+              cudaMemset(c.flags, 0, (L + 2) * sizeof(unsigned)) == cudaSuccess &&
               cudaMemset(c.status, 0, ST_COUNT * sizeof(int)) == cudaSuccess &&
               cudaMemset(c.c, 0, L * sizeof(cd)) == cudaSuccess && cudaMemset(c.x, 0, L * sizeof(cd)) == cudaSuccess;
     if (!ok) {

@@ -238,7 +238,7 @@ __device__ __forceinline__ void term_grad_plain(const double (&Lk)[N][N], const 
     }
     // ---- dV (matelem.f90:603-734) ----
     cd Qw[N][N];
-    coulomb_weights<N>(te.inv, sp, Qw);
+    coulomb_weights<N>(te, sp, Qw);
     cd WLk[NP], WBk[NP], WLl[NP], WBl[NP];
 #pragma unroll
     for (int x = 0; x < NP; x++) {
@@ -378,7 +378,7 @@ __device__ __forceinline__ void term_adjoint(const double (&P)[N][N], const cd (
     a_acc = rfma(coef, a, a_acc);
     // Qs = S/sqrt(pi) * Q
     cd Qw[N][N], Qs[N][N];
-    coulomb_weights<N>(te.inv, sp, Qw);
+    coulomb_weights<N>(te, sp, Qw);
     const cd sq = ONE_OVER_SQRTPI * S;
 #pragma unroll
     for (int i = 0; i < N; i++) {

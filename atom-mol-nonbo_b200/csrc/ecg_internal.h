@@ -67,6 +67,10 @@ struct Ctx {
     cd* zv = nullptr;           // D^-1 scaled forward result (ld)
     cd* spart = nullptr;        // per-CTA partial sums of the blocked solves
     double* colval = nullptr;   // per-column values of the quadratic forms (2 ld)
+    int* dblk = nullptr;        // device copy of blk_start + end (ld + 2 ints)
+    unsigned* flags = nullptr;  // per-panel ready flags of the cooperative solves (ld + 2)
+    unsigned epoch = 0;         // value a panel flag takes when its panel is solved
+    int coop_max_blocks = 0;    // co-resident CTAs of the cooperative solve kernels
     std::vector<int> blk_start; // block starts of the current LDL^H factor
     int fact_n = 0;             // rows covered by the current factor
 
@@ -83,6 +87,7 @@ struct Ctx {
 enum StatusWord {
     ST_ZERO_PIVOT = 0,   // first zero pivot row + 1 (0 = none)
     ST_NONFINITE = 1,    // a non-finite pair element was produced
+    ST_SOLVE_TIMEOUT = 2,  // a cooperative solve gave up waiting for a panel
     ST_COUNT = 8
 };
 

@@ -63,15 +63,25 @@ __device__ __forceinline__ cd rdiv(double r, cd b)
 }
 // Principal square root (branch cut on the negative real axis, as the
 // Fortran intrinsic): Kahan's formulation, "Branch cuts for complex
-// elementary functions" (1987).
-__device__ __forceinline__ cd csqrt(cd z)
+// elementary functions" (1987): t = sqrt((|x| + |z|)/2), then the other
+// component y/(2t).  One sqrt for |z| and one reciprocal square root give
+// both t and 1/t.  Also returns |z| (= |sqrt z|^2).
+__device__ __forceinline__ cd csqrt_r(cd z, double& absz)
 {
     const double r = sqrt(fma(z.x, z.x, z.y * z.y));
+    absz = r;
     if (r == 0.0) return cd{0.0, z.y};
-    const double t = sqrt(0.5 * (fabs(z.x) + r));
-    const double h = 0.5 * z.y / t;
+    const double u = 0.5 * (fabs(z.x) + r);
+    const double ri = rsqrt(u);
+    const double t = u * ri;
+    const double h = 0.5 * z.y * ri;
     if (z.x >= 0.0) return cd{t, h};
     return cd{fabs(h), copysign(t, z.y)};
+}
+__device__ __forceinline__ cd csqrt(cd z)
+{
+    double r;
+    return csqrt_r(z, r);
 }
 
 // Physical constants of one system: the n x n mass matrix
@@ -105,45 +115,54 @@ __host__ __device__ constexpr int vech_index(int N, int i, int j)
 // Per-term energy quantities shared by the energy, plain-gradient and
 // adjoint kernels.  Inputs: Ck = A_k - iB_k (bra, conjugated), tCl =
 // P'A_lP + iP'B_lP (permuted ket), absdet = |det L_k det L_l|.
-// Outputs: inv = C^-1 (symmetric), S, T, V as in src/matelem.f90:182-299.
+// Outputs: inv = C^-1 (symmetric), S, T, V as in src/matelem.f90:182-299,
+// and with CUBE the Coulomb cubes tr32[i][j] = tr[C^-1 J_ij]^(-3/2) of
+// src/matelem.f90:284-296 (diagonal: (C^-1_ii)^(-3/2)).
+// Divisions are folded into reciprocals: each pseudo-Cholesky pivot is
+// inverted once and reused by the factor and by its inverse, and
+// 1/sqrt(a) = conj(sqrt a)/|a|.
 template <int N>
 struct TermEnergy {
     cd inv[N][N];
     cd S, T, V;
+    cd tr32[N][N];
 };
 
-template <int N>
+template <int N, bool CUBE>
 __device__ __forceinline__ void term_energy(const cd (&Ck)[N][N], const cd (&tCl)[N][N], double absdet,
                                             const SysParams& sp, TermEnergy<N>& o)
 {
-    cd G[N][N];
+    cd G[N][N], rg[N];
     // pseudo-Cholesky C = G G^T of C = Ck + tCl (matelem.f90:203-217)
     cd det = mk(1.0, 0.0);
 #pragma unroll
     for (int i = 0; i < N; i++) {
+        {
+            cd s = Ck[i][i] + tCl[i][i];
 #pragma unroll
-        for (int j = i; j < N; j++) {
+            for (int k = i - 1; k >= 0; k--) s = cfms(G[i][k], G[i][k], s);
+            G[i][i] = csqrt(s);
+            det = det * s;
+            rg[i] = crcp(G[i][i]);
+        }
+#pragma unroll
+        for (int j = i + 1; j < N; j++) {
             cd s = Ck[i][j] + tCl[i][j];
 #pragma unroll
             for (int k = i - 1; k >= 0; k--) s = cfms(G[i][k], G[j][k], s);
-            if (i == j) {
-                G[i][i] = csqrt(s);
-                det = det * s;
-            } else {
-                G[j][i] = cdiv(s, G[i][i]);
-            }
+            G[j][i] = cmul(s, rg[i]);
         }
     }
     // X = G^-1 (lower) in place, then inv = X^T X (matelem.f90:221-241)
 #pragma unroll
     for (int i = 0; i < N; i++) {
-        G[i][i] = crcp(G[i][i]);
+        G[i][i] = rg[i];
 #pragma unroll
         for (int j = i + 1; j < N; j++) {
             cd s = mk(0.0, 0.0);
 #pragma unroll
             for (int k = i; k <= j - 1; k++) s = cfms(G[j][k], G[k][i], s);
-            G[j][i] = cdiv(s, G[j][j]);
+            G[j][i] = cmul(s, rg[j]);
         }
     }
 #pragma unroll
@@ -182,42 +201,51 @@ __device__ __forceinline__ void term_energy(const cd (&Ck)[N][N], const cd (&tCl
             tr = rfma(sp.M[i * NMAX + k], w2, tr);
         }
     o.T = 6.0 * (o.S * tr);
-    // Coulomb (matelem.f90:280-299)
+    // Coulomb (matelem.f90:280-299): cn / sqrt(a) = cn conj(sqrt a) / |a|
     const cd cn = TWO_OVER_SQRTPI * o.S;
     cd v = mk(0.0, 0.0);
 #pragma unroll
-    for (int i = 0; i < N; i++) v = rfma(sp.q[i], cdiv(cn, csqrt(o.inv[i][i])), v);
+    for (int i = 0; i < N; i++) {
+        const cd a = o.inv[i][i];
+        double r;
+        const cd sq = csqrt_r(a, r);
+        const double ir = 1.0 / r;
+        const cd is = mk(sq.x * ir, -sq.y * ir);  // 1/sqrt(a)
+        v = rfma(sp.q[i], cmul(cn, is), v);
+        if (CUBE) o.tr32[i][i] = cmul(is, mk(a.x * ir * ir, -a.y * ir * ir));  // a^(-1/2) a^(-1)
+    }
     v = sp.q0 * v;
 #pragma unroll
     for (int i = 0; i < N; i++)
 #pragma unroll
         for (int j = i + 1; j < N; j++) {
             const cd a = o.inv[i][i] + o.inv[j][j] - o.inv[j][i] - o.inv[j][i];
-            v = rfma(sp.q[i] * sp.q[j], cdiv(cn, csqrt(a)), v);
+            double r;
+            const cd sq = csqrt_r(a, r);
+            const double ir = 1.0 / r;
+            const cd is = mk(sq.x * ir, -sq.y * ir);
+            v = rfma(sp.q[i] * sp.q[j], cmul(cn, is), v);
+            if (CUBE) {
+                o.tr32[j][i] = cmul(is, mk(a.x * ir * ir, -a.y * ir * ir));
+                o.tr32[i][j] = o.tr32[j][i];
+            }
         }
     o.V = v;
 }
 
 // Coulomb weights for the gradient: cnumb_ij = q_i q_j tr[C^-1 J_ij]^(-3/2)
-// (i != j) and q0 q_i (C^-1_ii)^(-3/2) on the diagonal, as the
-// tr_inv_tCklJij32 array and cnumb of src/matelem.f90:284-296,677-681.
-// Returned in a symmetric matrix Qw[i][j].
+// (i != j) and q0 q_i (C^-1_ii)^(-3/2) on the diagonal, as cnumb of
+// src/matelem.f90:677-681, from the cubes kept by term_energy<N, true>.
 template <int N>
-__device__ __forceinline__ void coulomb_weights(const cd (&inv)[N][N], const SysParams& sp, cd (&Qw)[N][N])
+__device__ __forceinline__ void coulomb_weights(const TermEnergy<N>& te, const SysParams& sp, cd (&Qw)[N][N])
 {
 #pragma unroll
-    for (int i = 0; i < N; i++) {
-        const cd a = inv[i][i];
-        const cd r = crcp(csqrt(a) * a);
-        Qw[i][i] = (sp.q0 * sp.q[i]) * r;
-    }
+    for (int i = 0; i < N; i++) Qw[i][i] = (sp.q0 * sp.q[i]) * te.tr32[i][i];
 #pragma unroll
     for (int i = 0; i < N; i++)
 #pragma unroll
         for (int j = i + 1; j < N; j++) {
-            const cd a = inv[i][i] + inv[j][j] - inv[j][i] - inv[j][i];
-            const cd r = crcp(csqrt(a) * a);
-            Qw[j][i] = (sp.q[i] * sp.q[j]) * r;
+            Qw[j][i] = (sp.q[i] * sp.q[j]) * te.tr32[j][i];
             Qw[i][j] = Qw[j][i];
         }
 }

@@ -11,6 +11,7 @@
 // solved part; the last CTA to finish (atomic ticket, no waiting) sums the
 // partials in a fixed order and applies the panel's precomputed inverse
 // block, so results are deterministic run to run.
+#include <algorithm>
 #include "ecg_internal.h"
 
 namespace ecg {
@@ -146,6 +147,209 @@ __global__ void __launch_bounds__(256) k_bwd(const cd* __restrict__ A, int ld, i
     if (threadIdx.x == 0) *counter = 0;
 }
 
+// ---------------------------------------------------------------------------
+// Cooperative triangular solves: one CTA per LDL^H panel, all CTAs
+// co-resident (cooperative launch).  CTA j accumulates the contributions of
+// the panels it depends on in panel order, each as soon as that panel's
+// flag carries the current epoch (acquire / release), then applies its
+// inverse diagonal block and publishes its own panel.  Every wait is
+// bounded: after SOLVE_SPIN_LIMIT polls, or as soon as any CTA has given
+// up (the abort word), the CTA records ST_SOLVE_TIMEOUT and finishes
+// without waiting; the host then reports the step as failed.
+constexpr int SOLVE_SPIN_LIMIT = 1 << 22;
+constexpr int LS_LD = LDL_NB + 1;
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Wait (thread 0) for flags[a] == epoch; returns false if this CTA must stop.
+__device__ __forceinline__ bool wait_panel(const unsigned* flags, int a, unsigned epoch, int* status, int* abort_word,
+                                           bool& ok)
+{
+    __shared__ int go;
+    if (threadIdx.x == 0) {
+        int g = 1;
+        if (ok) {
+            int spins = 0;
+            while (ld_acquire(flags + a) != epoch) {
+                if (++spins > SOLVE_SPIN_LIMIT || *((volatile int*)abort_word) != 0) {
+                    g = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+            if (!g) {
+                atomicExch(status + ST_SOLVE_TIMEOUT, 1);
+                atomicExch(abort_word, 1);
+            }
+        } else {
+            g = 0;
+        }
+        go = g;
+    }
+    __syncthreads();
+    ok = ok && go;
+    return ok;
+}
+
+__device__ __forceinline__ void load_linv(const cd* __restrict__ linv, int j0, int b, double2* Ls)
+{
+    for (int e = threadIdx.x; e < LDL_NB * LDL_NB; e += blockDim.x) {
+        const int r = e / LDL_NB, q = e % LDL_NB;
+        double2 v = make_double2(0.0, 0.0);
+        if (r < b && q < b) {
+            const cd a = ld2(linv + (size_t)(j0 + r) * LDL_NB + q);
+            v = make_double2(a.x, a.y);
+        }
+        Ls[r * LS_LD + q] = v;
+    }
+}
+
+// Forward: y_j = Linv_j (w_j - sum_{a<j} U(a, j)^H y_a), z_j = invD_j y_j.
+__global__ void __launch_bounds__(256) k_fwd_coop(const cd* __restrict__ A, int ld, const int* __restrict__ bstart,
+                                                  int nb, const cd* __restrict__ w, cd* __restrict__ y,
+                                                  cd* __restrict__ z, const cd* __restrict__ invD,
+                                                  const cd* __restrict__ linv, unsigned* __restrict__ flags,
+                                                  unsigned epoch, int* __restrict__ status, int* abort_word)
+{
+    extern __shared__ double2 sm[];
+    double2* Ls = sm;                          // Linv_j, [r][q]
+    double2* red = sm + LDL_NB * LS_LD;        // [8][64] warp partials, then [4][64]
+    __shared__ double2 t[LDL_NB];
+    const int j = blockIdx.x;
+    const int j0 = bstart[j], j1 = bstart[j + 1], b = j1 - j0;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    load_linv(linv, j0, b, Ls);
+    // lane-partials for the 8 columns this warp owns
+    cd acc[8];
+#pragma unroll
+    for (int m = 0; m < 8; m++) acc[m] = mk(0.0, 0.0);
+    bool ok = true;
+    for (int a = 0; a < j; a++) {
+        if (!wait_panel(flags, a, epoch, status, abort_word, ok)) break;
+        const int a0 = bstart[a], a1 = bstart[a + 1];
+        const int r0 = a0 + lane, r1 = a0 + lane + 32;
+        const cd y0 = (r0 < a1) ? ldcg2(y + r0) : mk(0.0, 0.0);
+        const cd y1 = (r1 < a1) ? ldcg2(y + r1) : mk(0.0, 0.0);
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const int c = wp * 8 + m;
+            if (c < b) {
+                const cd* col = A + (size_t)(j0 + c) * ld;
+                if (r0 < a1) acc[m] = cfma(conj(ld2(col + r0)), y0, acc[m]);
+                if (r1 < a1) acc[m] = cfma(conj(ld2(col + r1)), y1, acc[m]);
+            }
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 8; m++) acc[m] = warp_sum(acc[m]);
+    if (lane == 0)
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const int c = wp * 8 + m;
+            if (c < b) t[c] = make_double2(0.0, 0.0), red[c] = make_double2(acc[m].x, acc[m].y);
+        }
+    __syncthreads();
+    if (threadIdx.x < b) {
+        const cd s = mk(red[threadIdx.x].x, red[threadIdx.x].y);
+        const cd v = ld2(w + j0 + threadIdx.x) - s;
+        t[threadIdx.x] = make_double2(v.x, v.y);
+    }
+    __syncthreads();
+    // y = Ls t: row r = tid & 63, four interleaved partial sums over q
+    {
+        const int r = threadIdx.x & 63, g = threadIdx.x >> 6;
+        cd s = mk(0.0, 0.0);
+        if (r < b)
+            for (int q = g; q <= r; q += 4) {
+                const double2 l = Ls[r * LS_LD + q], tq = t[q];
+                s = cfma(mk(l.x, l.y), mk(tq.x, tq.y), s);
+            }
+        red[g * LDL_NB + r] = make_double2(s.x, s.y);
+    }
+    __syncthreads();
+    if (threadIdx.x < b) {
+        const int r = threadIdx.x;
+        cd s = mk(0.0, 0.0);
+#pragma unroll
+        for (int g = 0; g < 4; g++) s = s + mk(red[g * LDL_NB + r].x, red[g * LDL_NB + r].y);
+        y[j0 + r] = s;
+        z[j0 + r] = cmul(s, ld2(invD + j0 + r));
+        __threadfence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) st_release(flags + j, epoch);
+}
+
+// Backward: x_j = Linv_j^H (z_j - sum_{c>j} U(j, c) x_c).
+__global__ void __launch_bounds__(256) k_bwd_coop(const cd* __restrict__ A, int ld, const int* __restrict__ bstart,
+                                                  int nb, const cd* __restrict__ z, cd* __restrict__ x,
+                                                  const cd* __restrict__ linv, unsigned* __restrict__ flags,
+                                                  unsigned epoch, int* __restrict__ status, int* abort_word)
+{
+    extern __shared__ double2 sm[];
+    double2* Ls = sm;
+    double2* red = sm + LDL_NB * LS_LD;  // [8][64]
+    __shared__ double2 t[LDL_NB];
+    const int j = blockIdx.x;
+    const int j0 = bstart[j], j1 = bstart[j + 1], b = j1 - j0;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    load_linv(linv, j0, b, Ls);
+    cd a0 = mk(0.0, 0.0), a1 = mk(0.0, 0.0);  // rows lane, lane + 32
+    bool ok = true;
+    for (int c = nb - 1; c > j; c--) {
+        if (!wait_panel(flags, c, epoch, status, abort_word, ok)) break;
+        const int c0 = bstart[c], c1 = bstart[c + 1];
+        for (int col = c0 + wp; col < c1; col += 8) {
+            const cd xc = ldcg2(x + col);
+            const cd* u = A + (size_t)col * ld + j0;
+            if (lane < b) a0 = cfma(ld2(u + lane), xc, a0);
+            if (lane + 32 < b) a1 = cfma(ld2(u + lane + 32), xc, a1);
+        }
+    }
+    red[wp * LDL_NB + lane] = make_double2(a0.x, a0.y);
+    red[wp * LDL_NB + lane + 32] = make_double2(a1.x, a1.y);
+    __syncthreads();
+    if (threadIdx.x < b) {
+        const int r = threadIdx.x;
+        cd s = mk(0.0, 0.0);
+#pragma unroll
+        for (int q = 0; q < 8; q++) s = s + mk(red[q * LDL_NB + r].x, red[q * LDL_NB + r].y);
+        const cd v = ld2(z + j0 + r) - s;
+        t[r] = make_double2(v.x, v.y);
+    }
+    __syncthreads();
+    {
+        const int r = threadIdx.x & 63, g = threadIdx.x >> 6;
+        cd s = mk(0.0, 0.0);
+        if (r < b)
+            for (int q = r + g; q < b; q += 4) {
+                const double2 l = Ls[q * LS_LD + r], tq = t[q];
+                s = cfma(conj(mk(l.x, l.y)), mk(tq.x, tq.y), s);
+            }
+        red[g * LDL_NB + r] = make_double2(s.x, s.y);
+    }
+    __syncthreads();
+    if (threadIdx.x < b) {
+        const int r = threadIdx.x;
+        cd s = mk(0.0, 0.0);
+#pragma unroll
+        for (int g = 0; g < 4; g++) s = s + mk(red[g * LDL_NB + r].x, red[g * LDL_NB + r].y);
+        x[j0 + r] = s;
+        __threadfence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) st_release(flags + j, epoch);
+}
+
 // Block-wide deterministic sums (1024 threads).
 template <int NV>
 __device__ __forceinline__ void block_sum(double (&v)[NV], double* sh)
@@ -269,10 +473,27 @@ __global__ void k_vec_scale(cd* __restrict__ v, int n, double s)
 }
 
 // ---------------------------------------------------------------------------
-int invit_step(Ctx& c, int n, bool /*first*/)
+static size_t coop_smem() { return (size_t)(LDL_NB * LS_LD + 8 * LDL_NB) * sizeof(double2); }
+
+// Largest grid the cooperative solves may use on this device (0: none).
+static int coop_capacity(Ctx& c)
 {
-    k_hemv<<<(n * 32 + 255) / 256, 256, 0, c.stream>>>(c.S, c.ld, n, c.c, c.w);
-    c.launches++;
+    if (c.coop_max_blocks) return c.coop_max_blocks;
+    const int sm = (int)coop_smem();
+    cudaFuncSetAttribute(k_fwd_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(k_bwd_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    int coop = 0, nsm = 0, per1 = 0, per2 = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c.dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, k_fwd_coop, 256, sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_bwd_coop, 256, sm);
+    cudaGetLastError();
+    c.coop_max_blocks = coop ? nsm * std::min(per1, per2) : -1;
+    return c.coop_max_blocks;
+}
+
+static int solve_multi_launch(Ctx& c, int n)
+{
     const int nb = (int)c.blk_start.size();
     for (int i = 0; i < nb; i++) {
         const int j0 = c.blk_start[i], j1 = (i + 1 < nb) ? c.blk_start[i + 1] : n;
@@ -293,6 +514,41 @@ int invit_step(Ctx& c, int n, bool /*first*/)
                                       c.counters + 1);
         c.launches++;
     }
+    return 0;
+}
+
+static int solve_cooperative(Ctx& c, int n)
+{
+    int nb = (int)c.blk_start.size();
+    const size_t sm = coop_smem();
+    int* abort_word = c.counters + 2;
+    if (cudaMemsetAsync(abort_word, 0, sizeof(int), c.stream) != cudaSuccess) return -2;
+    const int* bs = c.dblk;
+    const cd* H = c.H;
+    const cd* w = c.w;
+    const cd* invD = c.invD;
+    const cd* linv = c.linv;
+    int ld = c.ld;
+    unsigned e1 = ++c.epoch;
+    void* a1[] = {(void*)&H, &ld, (void*)&bs, &nb, (void*)&w, &c.yv, &c.zv, (void*)&invD, (void*)&linv, &c.flags,
+                  &e1, &c.status, &abort_word};
+    if (cudaLaunchCooperativeKernel((const void*)k_fwd_coop, nb, 256, a1, sm, c.stream) != cudaSuccess) return -2;
+    unsigned e2 = ++c.epoch;
+    const cd* zv = c.zv;
+    void* a2[] = {(void*)&H, &ld, (void*)&bs, &nb, (void*)&zv, &c.x, (void*)&linv, &c.flags, &e2, &c.status,
+                  &abort_word};
+    if (cudaLaunchCooperativeKernel((const void*)k_bwd_coop, nb, 256, a2, sm, c.stream) != cudaSuccess) return -2;
+    c.launches += 2;
+    return 0;
+}
+
+int invit_step(Ctx& c, int n, bool /*first*/)
+{
+    k_hemv<<<(n * 32 + 255) / 256, 256, 0, c.stream>>>(c.S, c.ld, n, c.c, c.w);
+    c.launches++;
+    const int nb = (int)c.blk_start.size();
+    int r = (nb <= coop_capacity(c)) ? solve_cooperative(c, n) : solve_multi_launch(c, n);
+    if (r) return r;
     k_iter_norm<<<1, 1024, 0, c.stream>>>(n, c.x, c.c, sqrt(2.0 * n), c.red);
     c.launches++;
     return cudaGetLastError() == cudaSuccess ? 0 : -2;

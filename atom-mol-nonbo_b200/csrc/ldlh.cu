@@ -57,32 +57,37 @@ __global__ void __launch_bounds__(256) k_ldl_mirror(cd* __restrict__ A, int ld, 
     }
 }
 
-// Diagonal block elimination.  Shared memory: W (b x b, upper used) and
-// X = L_pp^-1 (lower unit), both 64 x 64 complex.
+// Diagonal block elimination.  Shared memory: W (upper part used) and
+// X = L_pp^-1 (unit lower), both 64 x 65 complex (padded rows).  Thread
+// (ty, tx) of a 16 x 16 layout owns rows ty + 16i and columns tx + 16j of
+// both matrices, so each elimination step is a masked 4 x 4 update per
+// thread with no index arithmetic beyond shifts.
+constexpr int DG_LD = LDL_NB + 1;
 __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, int p0, int p1, cd* __restrict__ dw,
                                                    cd* __restrict__ invD, cd* __restrict__ linv,
                                                    int* __restrict__ status)
 {
     extern __shared__ double2 sm[];
-    double2* W = sm;                    // W[r*64 + c]
-    double2* X = sm + LDL_NB * LDL_NB;  // X[r*64 + s]
+    double2* W = sm;                   // W[r*DG_LD + c]
+    double2* X = sm + LDL_NB * DG_LD;  // X[r*DG_LD + s]
     __shared__ double2 u[LDL_NB];
     __shared__ double2 dws[LDL_NB];
     const int b = p1 - p0;
     const int tid = threadIdx.x;
+    const int ty = tid >> 4, tx = tid & 15;
     for (int e = tid; e < LDL_NB * LDL_NB; e += blockDim.x) {
-        const int r = e % LDL_NB, c = e / LDL_NB;
+        const int r = e & 63, c = e >> 6;
         double2 v = make_double2(0.0, 0.0);
         if (r < c && c < b) {
             const cd a = A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld];
             v = make_double2(a.x, a.y);
         }
-        W[r * LDL_NB + c] = v;
-        X[r * LDL_NB + c] = make_double2((r == c) ? 1.0 : 0.0, 0.0);
+        W[r * DG_LD + c] = v;
+        X[r * DG_LD + c] = make_double2((r == c) ? 1.0 : 0.0, 0.0);
     }
-    for (int r = tid; r < LDL_NB; r += blockDim.x) {
-        const cd d = (r < b) ? dw[p0 + r] : cd{1.0, 0.0};
-        dws[r] = make_double2(d.x, d.y);
+    if (tid < LDL_NB) {
+        const cd d = (tid < b) ? dw[p0 + tid] : cd{1.0, 0.0};
+        dws[tid] = make_double2(d.x, d.y);
     }
     __syncthreads();
     for (int q = 0; q < b; q++) {
@@ -92,59 +97,69 @@ __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, in
         const double nrm = dre * dre + dim * dim;
         double2 iq = make_double2(0.0, 0.0);
         if (nrm != 0.0) iq = make_double2(dre / nrm, -dim / nrm);
-        if (tid == 0) {
-            invD[p0 + q] = cd{iq.x, iq.y};
-            if (nrm == 0.0) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + q + 1);
-        }
-        for (int c = q + 1 + tid; c < b; c += blockDim.x) {
-            const double2 wv = W[q * LDL_NB + c];
-            u[c] = make_double2(wv.x * iq.x - wv.y * iq.y, wv.x * iq.y + wv.y * iq.x);
-        }
-        __syncthreads();
-        // trailing update inside the block (r <= c), diagonal into dws
-        const int m = b - q - 1;
-        for (int e = tid; e < m * m; e += blockDim.x) {
-            const int r = q + 1 + e / m, c = q + 1 + e % m;
-            if (r < c) {
-                const double2 ur = u[r], wq = W[q * LDL_NB + c];
-                double2 a = W[r * LDL_NB + c];
-                // a -= conj(U(q,r)) * W(q,c)
-                a.x -= ur.x * wq.x + ur.y * wq.y;
-                a.y -= ur.x * wq.y - ur.y * wq.x;
-                W[r * LDL_NB + c] = a;
-            } else if (r == c) {
-                const double2 uc = u[c], wq = W[q * LDL_NB + c];
-                double2 a = dws[c];
-                // dw -= conj(W(q,c)) * U(q,c)
-                a.x -= wq.x * uc.x + wq.y * uc.y;
-                a.y -= wq.x * uc.y - wq.y * uc.x;
-                dws[c] = a;
+        if (tid < LDL_NB) {
+            const int c = tid;
+            double2 uc = make_double2(0.0, 0.0);
+            if (c > q && c < b) {
+                const double2 wv = W[q * DG_LD + c];
+                uc = make_double2(wv.x * iq.x - wv.y * iq.y, wv.x * iq.y + wv.y * iq.x);
+            }
+            u[c] = uc;
+            if (tid == 0) {
+                invD[p0 + q] = cd{iq.x, iq.y};
+                if (nrm == 0.0) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + q + 1);
             }
         }
-        // X(r, s) -= L(r,q) X(q,s), L(r,q) = conj(U(q,r)), r > q, s <= q
-        for (int e = tid; e < m * (q + 1); e += blockDim.x) {
-            const int r = q + 1 + e / (q + 1), s = e % (q + 1);
-            const double2 ur = u[r], xq = X[q * LDL_NB + s];
-            double2 a = X[r * LDL_NB + s];
-            a.x -= ur.x * xq.x + ur.y * xq.y;
-            a.y -= ur.x * xq.y - ur.y * xq.x;
-            X[r * LDL_NB + s] = a;
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int r = ty + 16 * i;
+            if (r <= q || r >= b) continue;
+            const double2 ur = u[r];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int c = tx + 16 * j;
+                // W(r,c) -= conj(U(q,r)) W(q,c)   (r < c)
+                if (c > r && c < b) {
+                    const double2 wq = W[q * DG_LD + c];
+                    double2 a = W[r * DG_LD + c];
+                    a.x -= ur.x * wq.x + ur.y * wq.y;
+                    a.y -= ur.x * wq.y - ur.y * wq.x;
+                    W[r * DG_LD + c] = a;
+                } else if (c == r) {
+                    // dw -= conj(W(q,c)) U(q,c)
+                    const double2 wq = W[q * DG_LD + c];
+                    double2 a = dws[c];
+                    a.x -= wq.x * ur.x + wq.y * ur.y;
+                    a.y -= wq.x * ur.y - wq.y * ur.x;
+                    dws[c] = a;
+                }
+                // X(r,s) -= L(r,q) X(q,s), L(r,q) = conj(U(q,r)), s <= q
+                const int sc = c;
+                if (sc <= q) {
+                    const double2 xq = X[q * DG_LD + sc];
+                    double2 a = X[r * DG_LD + sc];
+                    a.x -= ur.x * xq.x + ur.y * xq.y;
+                    a.y -= ur.x * xq.y - ur.y * xq.x;
+                    X[r * DG_LD + sc] = a;
+                }
+            }
         }
         __syncthreads();
-        for (int c = q + 1 + tid; c < b; c += blockDim.x) W[q * LDL_NB + c] = u[c];
+        if (tid < LDL_NB && tid > q && tid < b) W[q * DG_LD + tid] = u[tid];
         __syncthreads();
     }
-    for (int e = tid; e < b * b; e += blockDim.x) {
-        const int r = e % b, c = e / b;
-        if (r < c) {
-            const double2 v = W[r * LDL_NB + c];
+    for (int e = tid; e < LDL_NB * LDL_NB; e += blockDim.x) {
+        const int r = e & 63, c = e >> 6;
+        if (r < c && c < b) {
+            const double2 v = W[r * DG_LD + c];
             A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld] = cd{v.x, v.y};
         }
     }
     for (int e = tid; e < b * LDL_NB; e += blockDim.x) {
-        const int r = e / LDL_NB, s = e % LDL_NB;
-        const double2 v = X[r * LDL_NB + s];
-        linv[(size_t)(p0 + r) * LDL_NB + s] = cd{v.x, v.y};
+        const int r = e >> 6, s2 = e & 63;
+        const double2 v = X[r * DG_LD + s2];
+        linv[(size_t)(p0 + r) * LDL_NB + s2] = cd{v.x, v.y};
     }
 }
 
@@ -306,7 +321,7 @@ int ldlh_factor(Ctx& c, int m0, int n)
     if (m0 > c.fact_n) return -1;
     if (!g_ldl_attr) {
         cudaFuncSetAttribute(k_ldl_diag, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(2 * LDL_NB * LDL_NB * sizeof(double2)));
+                             (int)(2 * LDL_NB * DG_LD * sizeof(double2)));
         cudaFuncSetAttribute(k_ldl_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(2 * LDL_NB * LDL_NB * sizeof(double2)));
         cudaFuncSetAttribute(k_ldl_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -338,7 +353,8 @@ int ldlh_factor(Ctx& c, int m0, int n)
         if (p1 <= p0) continue;
         const bool existing = (i < nexist);
         if (!existing) {
-            k_ldl_diag<<<1, 256, sm2, c.stream>>>(c.H, c.ld, p0, p1, c.dw, c.invD, c.linv, c.status);
+            k_ldl_diag<<<1, 256, 2 * LDL_NB * DG_LD * sizeof(double2), c.stream>>>(c.H, c.ld, p0, p1, c.dw, c.invD,
+                                                                                   c.linv, c.status);
             c.launches++;
         }
         const int clo = existing ? m0 : p1;
@@ -354,6 +370,12 @@ int ldlh_factor(Ctx& c, int m0, int n)
     if (cudaGetLastError() != cudaSuccess) return -2;
     c.blk_start = starts;
     c.fact_n = n;
+    // panel boundaries for the cooperative solves (starts..., n)
+    std::vector<int> bounds(starts);
+    bounds.push_back(n);
+    if (cudaMemcpyAsync(c.dblk, bounds.data(), bounds.size() * sizeof(int), cudaMemcpyHostToDevice, c.stream) !=
+        cudaSuccess)
+        return -2;
     return 0;
 }
 

@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(128) k_pair_diag(SysParams sp, const double* _
         cd tCl[N][N];
         load_sym<N>(ket + ((size_t)k * sp.T + t) * NP, tCl);
         TermEnergy<N> te;
-        term_energy<N>(Ck, tCl, absdet, sp, te);
+        term_energy<N, DERIV>(Ck, tCl, absdet, sp, te);
         const double cf = coef[t];
         Hs = rfma(cf, te.T + te.V, Hs);
         Ss = rfma(cf, te.S, Ss);
@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(256) k_pair_energy(SysParams sp, const double*
             cd tCl[N][N];
             load_sym<N>(ket + ((size_t)l * sp.T + t) * NP, tCl);
             TermEnergy<N> te;
-            term_energy<N>(Ck, tCl, absdet, sp, te);
+            term_energy<N, false>(Ck, tCl, absdet, sp, te);
             const double cf = __ldg(coef + t);
             Hs = rfma(cf, te.T + te.V, Hs);
             Ss = rfma(cf, te.S, Ss);
@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(NT) k_pair_grad(SysParams sp, const double* __
             cd tCl[N][N];
             load_sym<N>(ket + ((size_t)l * sp.T + t) * NP, tCl);
             TermEnergy<N> te;
-            term_energy<N>(Ck, tCl, absdet, sp, te);
+            term_energy<N, true>(Ck, tCl, absdet, sp, te);
             const double cf = __ldg(coef + t);
             Hs = rfma(cf, te.T + te.V, Hs);
             Ss = rfma(cf, te.S, Ss);
@@ -456,7 +456,7 @@ __global__ void __launch_bounds__(256) k_adjoint(SysParams sp, const double* __r
                 cd tCl[N][N];
                 load_sym<N>(ket + ((size_t)l * sp.T + t) * NP, tCl);
                 TermEnergy<N> te;
-                term_energy<N>(Ck, tCl, absdet, sp, te);
+                term_energy<N, true>(Ck, tCl, absdet, sp, te);
                 double P[N][N];
                 load_P<N>(Pd, t, P);
                 const double cf = __ldg(coef + t);
@@ -623,7 +623,7 @@ __global__ void __launch_bounds__(128) k_term_batch(SysParams sp, const double* 
     make_bra<N>(a, Ck, dk);
     make_ket<N>(b, P, tCl, dl);
     TermEnergy<N> te;
-    term_energy<N>(Ck, tCl, fabs(dl * dk), sp, te);
+    term_energy<N, true>(Ck, tCl, fabs(dl * dk), sp, te);
     hs[2 * (size_t)i] = te.T + te.V;
     hs[2 * (size_t)i + 1] = te.S;
     if (gradflag < 1 || gradflag > 3) return;

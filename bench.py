@@ -43,7 +43,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--K", type=int, default=None, help="override the basis size (testing only)")
-    ap.add_argument("--tol", type=float, default=1e-10, help="GHEPIIS tolerance (EIGVAL_TOLERANCE)")
+    ap.add_argument("--tol", type=float, default=-1e-6,
+                    help="GHEPIIS tolerance (EIGVAL_TOLERANCE); negative: iterate until the residual stops "
+                         "decreasing, once below |tol| (src/linalg.f90:1900-1906)")
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--cpu-baseline", type=int, default=1)
     ap.add_argument("--lam", type=float, default=None,

@@ -107,7 +107,9 @@ def test_deriv_matches_oracle(cfg, K, nfru):
         mask[i - nfru, : i + 1] = True
         mask[i - nfru, i:] = True
     kap = pair_conditions(sysm, params)
-    tolD = tolerance(kap[nfru:, :])  # (nfo, K): pair (function, partner)
+    # derivative vectors apply C^-1 twice (F = C^-1 tCl M tCl C^-1 and the
+    # Coulomb C^-1 J C^-1), so their rounding band is a few times wider
+    tolD = tolerance(kap[nfru:, :], c=256.0)  # (nfo, K): pair (function, partner)
     # each derivative vector relative to its largest entry
     scale = np.max(np.abs(Do), axis=0)
     r = np.abs(D - Do).max(axis=0) / (np.where(scale > 0, scale, 1.0) * tolD)

@@ -31,7 +31,8 @@ def test_matrix_elements_match_oracle(name, gradflag):
     with Context(sysm, 4) as ctx:
         H, S, Dk, Dl = ctx.matrix_elements(pk, pl, terms, gradflag)
     kap = term_conditions(sysm, pk, pl, terms)
-    tol = tolerance(kap)
+    # derivative vectors apply C^-1 twice, so their band is wider
+    tol = tolerance(kap, c=256.0 if gradflag else 64.0)
     worst, worst_ratio, n_tight = 0.0, 0.0, 0
     for i in range(cnt):
         h, s, dk, dl = o.matrix_elements(pk[i], pl[i], sysm.yhy_mats[terms[i]], gradflag)
