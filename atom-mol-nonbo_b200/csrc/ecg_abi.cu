@@ -1,6 +1,8 @@
 // ecg_abi.cu -- host side of libecgb200.so: context lifetime, the GHEPIIS
 // driver and the EnergyIA / EnergyIB glue behind the C ABI in ecg_abi.h.
 #include <float.h>
+#include <stdio.h>
+#include <stdlib.h>
 #include <math.h>
 #include <string.h>
 #include <algorithm>
@@ -31,6 +33,19 @@ namespace {
 
 constexpr int SOLVE_G_MAX = 64;
 
+// ECG_TRACE=1 in the environment prints the residual of every inverse
+// iteration to stderr (the reference's only convergence log is the
+// eigenvalue-tolerance bookkeeping of src/workproc.f90:1994-1995).
+bool trace_on()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char* e = getenv("ECG_TRACE");
+        on = (e && e[0] == '1') ? 1 : 0;
+    }
+    return on == 1;
+}
+
 template <typename T>
 int dalloc(T** p, size_t count)
 {
@@ -51,11 +66,17 @@ void free_ctx(Ctx& c)
                     c.zv, c.spart, c.colval, c.dblk, c.flags};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    for (auto& g : c.ldl_graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    c.ldl_graphs.clear();
+    if (c.bounds_h) cudaFreeHost(c.bounds_h);
     if (c.status_h) cudaFreeHost(c.status_h);
     if (c.red_h) cudaFreeHost(c.red_h);
     if (c.stream) {
         for (int i = 0; i < 16; i++) cudaEventDestroy(c.ev[i]);
         for (int i = 0; i < 2; i++) cudaEventDestroy(c.tev[i]);
+        for (int i = 0; i < 2; i++) cudaEventDestroy(c.lev[i]);
+        if (c.side) cudaStreamDestroy(c.side);
         cudaStreamDestroy(c.stream);
     }
 }
@@ -138,6 +159,7 @@ int ghepiis(Ctx& c, int k, int n, double apprlambda, double tol, int max_iter, i
         CKR(invit_step(c, n, it == 0));
         CKR(read_red(c));
         nd = c.red_h[RD_NORMDIFF];
+        if (trace_on()) fprintf(stderr, "ecg: GHEPIIS(%d,%d) iteration %d NormOfDiff %.3e\n", k, n, it + 1, nd);
         if (tol > 0.0) {
             if (nd <= tol) notconverged = false;
         } else {
@@ -290,6 +312,13 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
     }
     for (int i = 0; i < 16; i++) cudaEventCreate(&c.ev[i]);
     for (int i = 0; i < 2; i++) cudaEventCreate(&c.tev[i]);
+    for (int i = 0; i < 2; i++) cudaEventCreateWithFlags(&c.lev[i], cudaEventDisableTiming);
+    if (cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        free_ctx(c);
+        delete h;
+        return ECG_ECUDA;
+    }
     const size_t L = (size_t)ld;
     r |= dalloc(&c.params, (size_t)c.npt * L);
     r |= dalloc(&c.H, L * L);
@@ -310,7 +339,7 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
     r |= dalloc(&c.detL, L);
     r |= dalloc(&c.dw, L);
     r |= dalloc(&c.linv, L * LDL_NB);
-    r |= dalloc(&c.vbuf, L * LDL_NB);
+    r |= dalloc(&c.vbuf, 2 * L * LDL_NB);
     r |= dalloc(&c.status, (size_t)ST_COUNT);
     r |= dalloc(&c.red, (size_t)RD_COUNT);
     r |= dalloc(&c.counters, (size_t)4);
@@ -320,6 +349,7 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
     r |= dalloc(&c.flags, L + 2);
     if (!r) {
         if (cudaMallocHost((void**)&c.status_h, ST_COUNT * sizeof(int)) != cudaSuccess ||
+            cudaMallocHost((void**)&c.bounds_h, (L + 2) * sizeof(int)) != cudaSuccess ||
             cudaMallocHost((void**)&c.red_h, RD_COUNT * sizeof(double)) != cudaSuccess) {
             cudaGetLastError();
             r = ECG_ENOMEM;

@@ -29,6 +29,8 @@ struct Ctx {
     char method = 'I';   // 'I' (inverse iteration) or 'G' (generalised solver) storage
     SysParams sp{};
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;   // second stream of the LDL^H lookahead
+    cudaEvent_t lev[2];            // LDL^H lookahead events
 
     // Glob_* state, device resident
     double* params = nullptr;   // npt x ld, column-major (Glob_NonlinParam)
@@ -57,7 +59,7 @@ struct Ctx {
     // LDL^H workspace
     cd* dw = nullptr;           // working diagonal (ld)
     cd* linv = nullptr;         // ld x LDL_NB: inverse unit-lower diagonal blocks
-    cd* vbuf = nullptr;         // LDL_NB x ld: unscaled panel rows
+    cd* vbuf = nullptr;         // 2 x LDL_NB x ld: unscaled panel rows (ping-pong)
     int* status = nullptr;      // device status words (see ST_*)
     int* status_h = nullptr;    // pinned host mirror
     double* red = nullptr;      // reduction scratch for the solver (doubles)
@@ -72,6 +74,15 @@ struct Ctx {
     unsigned epoch = 0;         // value a panel flag takes when its panel is solved
     int coop_max_blocks = 0;    // co-resident CTAs of the cooperative solve kernels
     std::vector<int> blk_start; // block starts of the current LDL^H factor
+    // captured LDL^H factorisations, keyed by (m0, n, existing block starts)
+    struct LdlGraph {
+        std::vector<int> key;
+        cudaGraphExec_t exec = nullptr;
+        long long launches = 0;  // kernel launches one replay performs
+    };
+    long long graph_launches = 0;
+    std::vector<LdlGraph> ldl_graphs;
+    int* bounds_h = nullptr;    // pinned staging of the panel boundaries (ld + 2)
     int fact_n = 0;             // rows covered by the current factor
 
     // bookkeeping

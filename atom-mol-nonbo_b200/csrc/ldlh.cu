@@ -10,10 +10,11 @@
 // in the upper triangle, which holds the working Schur complement W(r,c),
 // r < c; the working diagonal lives in dw.  Per panel p = [p0,p1):
 //   k_ldl_diag    eliminate the 64 x 64 diagonal block in shared memory,
-//                 producing U (= L^H), invD and Linv = (U_pp^H)^-1;
-//   k_ldl_trsm    Wun(p, c) = Linv W(p, c), U(p, c) = invD Wun   (c beyond p);
+//                 producing U (= L^H) and invD;
+//   k_ldl_trsm    Wun(p, c) by substitution with U_pp, U(p, c) = invD Wun;
 //   k_ldl_update  W(r, c) -= sum_q conj(U(q,r)) Wun(q,c), r <= c beyond p
-//                 (the Hermitian rank-64 trailing update, a complex GEMM).
+//                 (the Hermitian rank-64 trailing update, a complex GEMM);
+//   k_ldl_linv    after the last panel: (U_pp^H)^-1 of every new panel.
 // The off-diagonal recurrence and the pivot d = conj(.) follow
 // src/linalg.f90:359-391 term for term; only the summation order differs.
 #include "ecg_internal.h"
@@ -57,104 +58,138 @@ __global__ void __launch_bounds__(256) k_ldl_mirror(cd* __restrict__ A, int ld, 
     }
 }
 
-// Diagonal block elimination.  Shared memory: W (upper part used) and
-// X = L_pp^-1 (unit lower), both 64 x 65 complex (padded rows).  Thread
-// (ty, tx) of a 16 x 16 layout owns rows ty + 16i and columns tx + 16j of
-// both matrices, so each elimination step is a masked 4 x 4 update per
-// thread with no index arithmetic beyond shifts.
+// Diagonal block elimination.  The working 64 x 64 tile lives in
+// registers: thread (ty, tx) of a 16 x 16 layout owns rows ty + 16i and
+// columns tx + 16j (16 complex values, the working diagonal included).  At
+// step q the owners of row q publish it to a double-buffered shared row, one
+// barrier later every thread applies the rank-one update to its elements
+// (W(r,c) -= conj(U(q,r)) W(q,c), r < c; dw(c) -= conj(W(q,c)) U(q,c)), and
+// the row-q owners keep U(q,.) = invD_q W(q,.).
 constexpr int DG_LD = LDL_NB + 1;
 __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, int p0, int p1, cd* __restrict__ dw,
-                                                   cd* __restrict__ invD, cd* __restrict__ linv,
-                                                   int* __restrict__ status)
+                                                   cd* __restrict__ invD, int* __restrict__ status)
 {
-    extern __shared__ double2 sm[];
-    double2* W = sm;                   // W[r*DG_LD + c]
-    double2* X = sm + LDL_NB * DG_LD;  // X[r*DG_LD + s]
-    __shared__ double2 u[LDL_NB];
-    __shared__ double2 dws[LDL_NB];
+    __shared__ double2 rowq[2][LDL_NB];
     const int b = p1 - p0;
     const int tid = threadIdx.x;
     const int ty = tid >> 4, tx = tid & 15;
-    for (int e = tid; e < LDL_NB * LDL_NB; e += blockDim.x) {
-        const int r = e & 63, c = e >> 6;
-        double2 v = make_double2(0.0, 0.0);
-        if (r < c && c < b) {
-            const cd a = A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld];
-            v = make_double2(a.x, a.y);
+    cd w[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int r = ty + 16 * i, c = tx + 16 * j;
+            cd v = cd{0.0, 0.0};
+            if (r < b && c < b) {
+                if (r < c)
+                    v = A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld];
+                else if (r == c)
+                    v = dw[p0 + r];
+            }
+            w[i][j] = v;
         }
-        W[r * DG_LD + c] = v;
-        X[r * DG_LD + c] = make_double2((r == c) ? 1.0 : 0.0, 0.0);
-    }
-    if (tid < LDL_NB) {
-        const cd d = (tid < b) ? dw[p0 + tid] : cd{1.0, 0.0};
-        dws[tid] = make_double2(d.x, d.y);
-    }
-    __syncthreads();
     for (int q = 0; q < b; q++) {
-        // pivot d = conj(dw_q) (src/linalg.f90:375-383)
-        const double2 dq = dws[q];
-        const double dre = dq.x, dim = -dq.y;
-        const double nrm = dre * dre + dim * dim;
-        double2 iq = make_double2(0.0, 0.0);
-        if (nrm != 0.0) iq = make_double2(dre / nrm, -dim / nrm);
-        if (tid < LDL_NB) {
-            const int c = tid;
-            double2 uc = make_double2(0.0, 0.0);
-            if (c > q && c < b) {
-                const double2 wv = W[q * DG_LD + c];
-                uc = make_double2(wv.x * iq.x - wv.y * iq.y, wv.x * iq.y + wv.y * iq.x);
-            }
-            u[c] = uc;
-            if (tid == 0) {
-                invD[p0 + q] = cd{iq.x, iq.y};
-                if (nrm == 0.0) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + q + 1);
-            }
+        double2* rq = rowq[q & 1];
+        if ((q & 15) == ty) {
+            const int iq = q >> 4;
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                if (i == iq)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) rq[tx + 16 * j] = make_double2(w[i][j].x, w[i][j].y);
         }
         __syncthreads();
+        // pivot d = conj(dw_q), invD = 1/d (src/linalg.f90:375-383)
+        const double2 dq = rq[q];
+        const double nrm = dq.x * dq.x + dq.y * dq.y;
+        const double inrm = (nrm != 0.0) ? 1.0 / nrm : 0.0;
+        const cd iq = cd{dq.x * inrm, dq.y * inrm};  // 1 / conj(dw_q)
+        if (tid == 0) {
+            invD[p0 + q] = iq;
+            if (nrm == 0.0) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + q + 1);
+        }
+        cd wq[4];  // unscaled W(q, c) of this thread's columns
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const double2 v = rq[tx + 16 * j];
+            wq[j] = cd{v.x, v.y};
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int r = ty + 16 * i;
+            if (r > q && r < b) {
+                const double2 v = rq[r];
+                const cd cu = conj(cmul(cd{v.x, v.y}, iq));  // conj(U(q, r))
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int c = tx + 16 * j;
+                    // W(r,c) -= conj(U(q,r)) W(q,c)
+                    if (c > r && c < b) w[i][j] = cfms(cu, wq[j], w[i][j]);
+                }
+                // diagonal (c == r iff tx == ty, j == i): dw -= conj(W(q,r)) U(q,r)
+                if (tx == ty) w[i][i] = cfms(cd{v.x, -v.y}, conj(cu), w[i][i]);
+            } else if (r == q) {
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int c = tx + 16 * j;
+                    if (c > q && c < b) w[i][j] = cmul(wq[j], iq);  // U(q, c)
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int r = ty + 16 * i, c = tx + 16 * j;
+            if (r < c && c < b) A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld] = w[i][j];
+        }
+}
+
+// Inverse of the unit lower diagonal block L_pp = U_pp^H of every panel in
+// [first, nb) (one CTA per panel, all independent): Gaussian elimination of
+// L applied to the identity, X(r,s) -= L(r,q) X(q,s).  Row r of X lands in
+// linv[(p0 + r) * 64 + s]; the triangular solves of the inverse iteration
+// apply these blocks instead of substituting row by row.
+__global__ void __launch_bounds__(256) k_ldl_linv(const cd* __restrict__ A, int ld, const int* __restrict__ bstart,
+                                                   int first, cd* __restrict__ linv)
+{
+    extern __shared__ double2 sm[];
+    double2* U = sm;                   // U[q*DG_LD + r] = U(q, r), q < r
+    double2* X = sm + LDL_NB * DG_LD;  // X[r*DG_LD + s]
+    const int blk = first + blockIdx.x;
+    const int p0 = bstart[blk], p1 = bstart[blk + 1], b = p1 - p0;
+    const int tid = threadIdx.x;
+    const int ty = tid >> 4, tx = tid & 15;
+    for (int e = tid; e < LDL_NB * LDL_NB; e += blockDim.x) {
+        const int q = e & 63, r = e >> 6;
+        double2 v = make_double2(0.0, 0.0);
+        if (q < r && r < b) {
+            const cd a = A[(size_t)(p0 + q) + (size_t)(p0 + r) * ld];
+            v = make_double2(a.x, a.y);
+        }
+        U[q * DG_LD + r] = v;
+        X[q * DG_LD + r] = make_double2((q == r) ? 1.0 : 0.0, 0.0);
+    }
+    __syncthreads();
+    for (int q = 0; q + 1 < b; q++) {
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             const int r = ty + 16 * i;
             if (r <= q || r >= b) continue;
-            const double2 ur = u[r];
+            const double2 ur = U[q * DG_LD + r];  // L(r,q) = conj(U(q,r))
 #pragma unroll
             for (int j = 0; j < 4; j++) {
-                const int c = tx + 16 * j;
-                // W(r,c) -= conj(U(q,r)) W(q,c)   (r < c)
-                if (c > r && c < b) {
-                    const double2 wq = W[q * DG_LD + c];
-                    double2 a = W[r * DG_LD + c];
-                    a.x -= ur.x * wq.x + ur.y * wq.y;
-                    a.y -= ur.x * wq.y - ur.y * wq.x;
-                    W[r * DG_LD + c] = a;
-                } else if (c == r) {
-                    // dw -= conj(W(q,c)) U(q,c)
-                    const double2 wq = W[q * DG_LD + c];
-                    double2 a = dws[c];
-                    a.x -= wq.x * ur.x + wq.y * ur.y;
-                    a.y -= wq.x * ur.y - wq.y * ur.x;
-                    dws[c] = a;
-                }
-                // X(r,s) -= L(r,q) X(q,s), L(r,q) = conj(U(q,r)), s <= q
-                const int sc = c;
-                if (sc <= q) {
-                    const double2 xq = X[q * DG_LD + sc];
-                    double2 a = X[r * DG_LD + sc];
-                    a.x -= ur.x * xq.x + ur.y * xq.y;
-                    a.y -= ur.x * xq.y - ur.y * xq.x;
-                    X[r * DG_LD + sc] = a;
-                }
+                const int sc = tx + 16 * j;
+                if (sc > q) continue;
+                const double2 xq = X[q * DG_LD + sc];
+                double2 a = X[r * DG_LD + sc];
+                a.x -= ur.x * xq.x + ur.y * xq.y;
+                a.y -= ur.x * xq.y - ur.y * xq.x;
+                X[r * DG_LD + sc] = a;
             }
         }
         __syncthreads();
-        if (tid < LDL_NB && tid > q && tid < b) W[q * DG_LD + tid] = u[tid];
-        __syncthreads();
-    }
-    for (int e = tid; e < LDL_NB * LDL_NB; e += blockDim.x) {
-        const int r = e & 63, c = e >> 6;
-        if (r < c && c < b) {
-            const double2 v = W[r * DG_LD + c];
-            A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld] = cd{v.x, v.y};
-        }
     }
     for (int e = tid; e < b * LDL_NB; e += blockDim.x) {
         const int r = e >> 6, s2 = e & 63;
@@ -163,219 +198,322 @@ __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, in
     }
 }
 
-// Panel rows: Wun(p, c) = Linv W(p, c); U(p, c) = invD Wun; vbuf(., c) = Wun.
-// One CTA per 64 columns; 256 threads, each 4 rows x 4 columns.
+// Panel rows beyond the diagonal block, by substitution:
+//   Wun(q, c) = W(q, c) - sum_{q' < q} conj(U(q', q)) Wun(q', c)
+//   U(q, c)   = invD_q Wun(q, c);  vbuf(q, c) = Wun(q, c)
+// (the forward form of src/linalg.f90:384-389 for a whole panel).  One warp
+// per column, lanes hold rows lane and lane + 32; U_pp comes from A through
+// shared memory.  32 columns per CTA.
+constexpr int TRSM_COLS = 8;
 __global__ void __launch_bounds__(256) k_ldl_trsm(cd* __restrict__ A, int ld, int p0, int p1, int c0, int n,
-                                                   const cd* __restrict__ invD, const cd* __restrict__ linv,
-                                                   cd* __restrict__ vbuf)
+                                                   const cd* __restrict__ invD, cd* __restrict__ vbuf)
 {
     extern __shared__ double2 sm[];
-    double2* Ls = sm;                     // Ls[q*64 + r] = Linv(r, q)
-    double2* Ws = sm + LDL_NB * LDL_NB;   // Ws[q*64 + c]
+    double2* U = sm;  // U[q*DG_LD + r] = U(q, r), q < r
     const int b = p1 - p0;
-    const int cbase = c0 + blockIdx.x * LDL_NB;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
     for (int e = tid; e < LDL_NB * LDL_NB; e += blockDim.x) {
-        const int s = e % LDL_NB, r = e / LDL_NB;
-        double2 v = make_double2(0.0, 0.0);
-        if (r < b && s < b) {
-            const cd a = ldg2(linv + (size_t)(p0 + r) * LDL_NB + s);
-            v = make_double2(a.x, a.y);
+        const int q = e & 63, r = e >> 6;
+        if (q < r && r < b) {
+            const cd a = A[(size_t)(p0 + q) + (size_t)(p0 + r) * ld];
+            U[q * DG_LD + r] = make_double2(a.x, a.y);
         }
-        Ls[s * LDL_NB + r] = v;
-    }
-    for (int e = tid; e < LDL_NB * LDL_NB; e += blockDim.x) {
-        const int q = e % LDL_NB, cc = e / LDL_NB;
-        const int c = cbase + cc;
-        double2 v = make_double2(0.0, 0.0);
-        if (q < b && c < n) {
-            const cd a = A[(size_t)(p0 + q) + (size_t)c * ld];
-            v = make_double2(a.x, a.y);
-        }
-        Ws[q * LDL_NB + cc] = v;
     }
     __syncthreads();
-    const int tr = tid % 16, tc = tid / 16;
-    double2 acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = make_double2(0.0, 0.0);
-    for (int q = 0; q < b; q++) {
-        double2 a[4], w[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) a[i] = Ls[q * LDL_NB + tr + 16 * i];
-#pragma unroll
-        for (int j = 0; j < 4; j++) w[j] = Ws[q * LDL_NB + tc + 16 * j];
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                acc[i][j].x = fma(a[i].x, w[j].x, fma(-a[i].y, w[j].y, acc[i][j].x));
-                acc[i][j].y = fma(a[i].x, w[j].y, fma(a[i].y, w[j].x, acc[i][j].y));
+    const int r0 = lane, r1 = lane + 32;
+    const cd d0 = (r0 < b) ? invD[p0 + r0] : cd{0.0, 0.0};
+    const cd d1 = (r1 < b) ? invD[p0 + r1] : cd{0.0, 0.0};
+    for (int m = 0; m < TRSM_COLS / 8; m++) {
+        const int c = c0 + blockIdx.x * TRSM_COLS + wp * (TRSM_COLS / 8) + m;  // one column per warp
+        if (c >= n) break;
+        cd* col = A + (size_t)c * ld + p0;
+        cd w0 = (r0 < b) ? col[r0] : cd{0.0, 0.0};
+        cd w1 = (r1 < b) ? col[r1] : cd{0.0, 0.0};
+        for (int q = 0; q < b; q++) {
+            // broadcast the finished row q
+            const cd src = (q < 32) ? w0 : w1;
+            cd wq;
+            wq.x = __shfl_sync(0xffffffffu, src.x, q & 31);
+            wq.y = __shfl_sync(0xffffffffu, src.y, q & 31);
+            if (r0 > q && r0 < b) {
+                const double2 uq = U[q * DG_LD + r0];
+                w0 = cfms(cd{uq.x, -uq.y}, wq, w0);
             }
-    }
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int r = tr + 16 * i;
-        if (r >= b) continue;
-        const cd id = invD[p0 + r];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int c = cbase + tc + 16 * j;
-            if (c >= n) continue;
-            const double2 v = acc[i][j];
-            vbuf[(size_t)r + (size_t)c * LDL_NB] = cd{v.x, v.y};
-            A[(size_t)(p0 + r) + (size_t)c * ld] = cd{v.x * id.x - v.y * id.y, v.x * id.y + v.y * id.x};
+            if (r1 > q && r1 < b) {
+                const double2 uq = U[q * DG_LD + r1];
+                w1 = cfms(cd{uq.x, -uq.y}, wq, w1);
+            }
+        }
+        cd* v = vbuf + (size_t)c * LDL_NB;
+        if (r0 < b) {
+            v[r0] = w0;
+            col[r0] = cmul(w0, d0);
+        }
+        if (r1 < b) {
+            v[r1] = w1;
+            col[r1] = cmul(w1, d1);
         }
     }
 }
 
-// Trailing update over 64 x 64 output tiles: rows r in [r0, n), columns
-// c in [max(r, c0), n).  K-chunks of 32 panel rows through shared memory.
+// Trailing update over 64 x 64 output tiles on the FP64 tensor cores:
+//   W(r, c) -= sum_q conj(U(q, r)) Wun(q, c),  r in [r0, rend), c in [max(r, c0), n)
+// with mma.sync.m8n8k4.f64.  Eight warps as 2 x 4, each a 32 x 16 complex
+// sub-tile (4 x 2 tiles of 8 x 8); per tile and k-step of 4 the real and
+// imaginary accumulators take four mma: Re += Ur Vr + Ui Vi and
+// Im += Ur Vi + (-Ui) Vr (the conjugate folded into a negated fragment).
+// Panel rows are staged through shared memory in chunks of 32 with real and
+// imaginary parts in separate arrays (row pitch 68 doubles: the four k rows
+// of a fragment load fall in distinct banks).
 constexpr int UPD_KC = 32;
-constexpr int UPD_LD = LDL_NB + 1;  // padded row of the shared tiles
-__global__ void __launch_bounds__(256) k_ldl_update(cd* __restrict__ A, int ld, int p0, int p1, int r0, int c0,
-                                                     int n, const cd* __restrict__ vbuf, cd* __restrict__ dw)
+constexpr int UPD_LD = 68;
+constexpr size_t UPD_SMEM = 4 * UPD_KC * UPD_LD * sizeof(double);
+
+__device__ __forceinline__ void mma_f64(double& c0, double& c1, double a, double b)
 {
-    extern __shared__ double2 sm[];
-    double2(*Us)[UPD_LD] = reinterpret_cast<double2(*)[UPD_LD]>(sm);                   // U(q, r)
-    double2(*Vs)[UPD_LD] = reinterpret_cast<double2(*)[UPD_LD]>(sm + UPD_KC * UPD_LD);  // Wun(q, c)
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+template <int TC, int WR, int WC>
+__global__ void __launch_bounds__(256) k_ldl_update(cd* __restrict__ A, int ld, int p0, int p1, int r0, int rend,
+                                                     int c0, int n, const cd* __restrict__ vbuf, cd* __restrict__ dw)
+{
+    constexpr int MT = LDL_NB / WR / 8;  // 8 x 8 tiles per warp along rows
+    constexpr int NT = TC / WC / 8;      // and along columns
+    extern __shared__ double smd[];
+    double* Ur = smd;                       // [k][m]
+    double* Ui = Ur + UPD_KC * UPD_LD;
+    double* Vr = Ui + UPD_KC * UPD_LD;      // [k][n]
+    double* Vi = Vr + UPD_KC * UPD_LD;
     const int rb = r0 + blockIdx.y * LDL_NB;
-    const int cb = c0 + blockIdx.x * LDL_NB;
-    if (rb > cb + LDL_NB - 1) return;  // tile entirely below the diagonal
+    const int cb = c0 + blockIdx.x * TC;
+    if (rb > cb + TC - 1) return;  // tile entirely below the diagonal
     const int b = p1 - p0;
-    const int tid = threadIdx.x;
-    const int tr = tid % 16, tc = tid / 16;
-    double2 acc[4][4];
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    const int wr = wp / WC, wc = wp % WC;  // warp rows MT*8*wr, columns NT*8*wc
+    const int g = lane >> 2, t4 = lane & 3;
+    double accr[MT][NT][2], acci[MT][NT][2];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+    for (int mt = 0; mt < MT; mt++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = make_double2(0.0, 0.0);
+        for (int nt = 0; nt < NT; nt++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) accr[mt][nt][e] = acci[mt][nt][e] = 0.0;
     for (int k0 = 0; k0 < b; k0 += UPD_KC) {
         for (int e = tid; e < UPD_KC * LDL_NB; e += blockDim.x) {
-            const int q = e % UPD_KC, rr = e / UPD_KC;
-            const int r = rb + rr, c = cb + rr;
-            double2 u = make_double2(0.0, 0.0), v = make_double2(0.0, 0.0);
-            if (k0 + q < b) {
-                if (r < n) {
-                    const cd a = A[(size_t)(p0 + k0 + q) + (size_t)r * ld];
-                    u = make_double2(a.x, a.y);
-                }
-                if (c < n) {
-                    const cd a = ldg2(vbuf + (size_t)(k0 + q) + (size_t)c * LDL_NB);
-                    v = make_double2(a.x, a.y);
-                }
-            }
-            Us[q][rr] = u;
-            Vs[q][rr] = v;
+            const int q = e % UPD_KC, mm = e / UPD_KC;
+            const int r = rb + mm;
+            cd u = cd{0.0, 0.0};
+            if (k0 + q < b && r < rend) u = A[(size_t)(p0 + k0 + q) + (size_t)r * ld];
+            Ur[q * UPD_LD + mm] = u.x;
+            Ui[q * UPD_LD + mm] = u.y;
+        }
+        for (int e = tid; e < UPD_KC * TC; e += blockDim.x) {
+            const int q = e % UPD_KC, mm = e / UPD_KC;
+            const int c = cb + mm;
+            cd v = cd{0.0, 0.0};
+            if (k0 + q < b && c < n) v = ldg2(vbuf + (size_t)(k0 + q) + (size_t)c * LDL_NB);
+            Vr[q * UPD_LD + mm] = v.x;
+            Vi[q * UPD_LD + mm] = v.y;
         }
         __syncthreads();
-#pragma unroll 4
-        for (int q = 0; q < UPD_KC; q++) {
-            double2 a[4], w[4];
+#pragma unroll 2
+        for (int kk = 0; kk < UPD_KC; kk += 4) {
+            const int kr = (kk + t4) * UPD_LD;
+            double ar[MT], ai[MT], br[NT], bi[NT];
 #pragma unroll
-            for (int i = 0; i < 4; i++) a[i] = Us[q][tr + 16 * i];
+            for (int mt = 0; mt < MT; mt++) {
+                const int m = (wr * MT + mt) * 8 + g;
+                ar[mt] = Ur[kr + m];
+                ai[mt] = Ui[kr + m];
+            }
 #pragma unroll
-            for (int j = 0; j < 4; j++) w[j] = Vs[q][tc + 16 * j];
+            for (int nt = 0; nt < NT; nt++) {
+                const int nn = (wc * NT + nt) * 8 + g;
+                br[nt] = Vr[kr + nn];
+                bi[nt] = Vi[kr + nn];
+            }
 #pragma unroll
-            for (int i = 0; i < 4; i++)
+            for (int mt = 0; mt < MT; mt++)
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    // acc += conj(a) * w
-                    acc[i][j].x = fma(a[i].x, w[j].x, fma(a[i].y, w[j].y, acc[i][j].x));
-                    acc[i][j].y = fma(a[i].x, w[j].y, fma(-a[i].y, w[j].x, acc[i][j].y));
+                for (int nt = 0; nt < NT; nt++) {
+                    mma_f64(accr[mt][nt][0], accr[mt][nt][1], ar[mt], br[nt]);
+                    mma_f64(accr[mt][nt][0], accr[mt][nt][1], ai[mt], bi[nt]);
+                    mma_f64(acci[mt][nt][0], acci[mt][nt][1], ar[mt], bi[nt]);
+                    mma_f64(acci[mt][nt][0], acci[mt][nt][1], -ai[mt], br[nt]);
                 }
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int r = rb + tr + 16 * i;
-        if (r >= n) continue;
+    for (int mt = 0; mt < MT; mt++) {
+        const int r = rb + (wr * MT + mt) * 8 + g;
+        if (r >= rend) continue;
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int c = cb + tc + 16 * j;
-            if (c >= n || c < r) continue;
-            const double2 v = acc[i][j];
-            if (c == r) {
-                // dw -= conj(sum conj(U) Wun) = sum conj(Wun) U (src/linalg.f90:370-372)
-                cd d = dw[c];
-                d.x -= v.x;
-                d.y += v.y;
-                dw[c] = d;
-            } else {
-                cd& a = A[(size_t)r + (size_t)c * ld];
-                a.x -= v.x;
-                a.y -= v.y;
+        for (int nt = 0; nt < NT; nt++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int c = cb + (wc * NT + nt) * 8 + t4 * 2 + e;
+                if (c >= n || c < r) continue;
+                const double vr = accr[mt][nt][e], vi = acci[mt][nt][e];
+                if (c == r) {
+                    // dw -= conj(sum conj(U) Wun) = sum conj(Wun) U (src/linalg.f90:370-372)
+                    cd d = dw[c];
+                    d.x -= vr;
+                    d.y += vi;
+                    dw[c] = d;
+                } else {
+                    cd& a = A[(size_t)r + (size_t)c * ld];
+                    a.x -= vr;
+                    a.y -= vi;
+                }
             }
-        }
     }
 }
 
 static bool g_ldl_attr = false;
 
-int ldlh_factor(Ctx& c, int m0, int n)
+// Trailing update by panel [p0, p1) of rows [r0, rend), columns
+// [max(r, c0), n).
+static void launch_update(Ctx& c, cudaStream_t st, const cd* vb, int p0, int p1, int r0, int rend, int c0, int n)
 {
-    if (m0 < 0 || m0 > n || n > c.ld) return -1;
-    if (m0 > c.fact_n) return -1;
-    if (!g_ldl_attr) {
-        cudaFuncSetAttribute(k_ldl_diag, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(2 * LDL_NB * DG_LD * sizeof(double2)));
-        cudaFuncSetAttribute(k_ldl_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(2 * LDL_NB * LDL_NB * sizeof(double2)));
-        cudaFuncSetAttribute(k_ldl_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(2 * UPD_KC * UPD_LD * sizeof(double2)));
-        g_ldl_attr = true;
+    if (rend <= r0 || c0 >= n) return;
+    const int nrb = (rend - r0 + LDL_NB - 1) / LDL_NB;
+    if (nrb == 1) {
+        // one panel of rows (the lookahead rows): narrow 64 x 16 tiles so
+        // that enough CTAs run
+        dim3 g((n - c0 + 15) / 16, 1);
+        k_ldl_update<16, 8, 1><<<g, 256, UPD_SMEM, st>>>(c.H, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
+    } else {
+        dim3 g((n - c0 + LDL_NB - 1) / LDL_NB, nrb);
+        k_ldl_update<64, 2, 4><<<g, 256, UPD_SMEM, st>>>(c.H, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
     }
-    const size_t upd_sm = 2 * UPD_KC * UPD_LD * sizeof(double2);
-    // block list: existing blocks truncated at m0, then new 64-row blocks
-    std::vector<int> starts;
-    for (int s : c.blk_start)
-        if (s < m0) starts.push_back(s);
-    const int nexist = (int)starts.size();
-    for (int s = m0; s < n; s += LDL_NB) starts.push_back(s);
+    c.launches++;
+}
+
+// Enqueue the kernels of one factorisation (see ldlh_factor).
+static void enqueue_factor(Ctx& c, int m0, int n, const std::vector<int>& starts, int nexist)
+{
+    const size_t sm1 = LDL_NB * DG_LD * sizeof(double2);
     const int nblk = (int)starts.size();
-    auto blk_end = [&](int i) {
-        if (i + 1 < nblk) return starts[i + 1];
-        return n;
-    };
+    auto blk_end = [&](int i) { return (i + 1 < nblk) ? starts[i + 1] : n; };
     if (n > m0) {
         const int ct0 = m0 / 32, ct1 = (n + 31) / 32;
         dim3 g(ct1 - ct0, ct1);
         k_ldl_mirror<<<g, 256, 0, c.stream>>>(c.H, c.ld, m0, n, c.dw, ct0);
         c.launches++;
     }
-    const size_t sm2 = 2 * LDL_NB * LDL_NB * sizeof(double2);
-    for (int i = 0; i < nblk; i++) {
-        const int p0 = starts[i];
-        const int p1 = (i < nexist) ? std::min(blk_end(i), m0) : blk_end(i);
-        if (p1 <= p0) continue;
-        const bool existing = (i < nexist);
-        if (!existing) {
-            k_ldl_diag<<<1, 256, 2 * LDL_NB * DG_LD * sizeof(double2), c.stream>>>(c.H, c.ld, p0, p1, c.dw, c.invD,
-                                                                                   c.linv, c.status);
-            c.launches++;
-        }
-        const int clo = existing ? m0 : p1;
-        if (clo >= n) continue;
-        const int ncb = (n - clo + LDL_NB - 1) / LDL_NB;
-        k_ldl_trsm<<<ncb, 256, sm2, c.stream>>>(c.H, c.ld, p0, p1, clo, n, c.invD, c.linv, c.vbuf);
+    // existing panels (bordered update): apply them to the new columns in order
+    for (int i = 0; i < nexist; i++) {
+        const int p0 = starts[i], p1 = std::min(blk_end(i), m0);
+        if (p1 <= p0 || m0 >= n) continue;
+        k_ldl_trsm<<<(n - m0 + TRSM_COLS - 1) / TRSM_COLS, 256, sm1, c.stream>>>(c.H, c.ld, p0, p1, m0, n, c.invD,
+                                                                                c.vbuf);
         c.launches++;
-        const int nrb = (n - p1 + LDL_NB - 1) / LDL_NB;
-        dim3 g(ncb, nrb);
-        k_ldl_update<<<g, 256, upd_sm, c.stream>>>(c.H, c.ld, p0, p1, p1, clo, n, c.vbuf, c.dw);
+        launch_update(c, c.stream, c.vbuf, p0, p1, p1, n, m0, n);
+    }
+    // new panels, right-looking with a depth-one lookahead: the rows of the
+    // next panel are updated first on the main stream, so that panel's
+    // factorisation overlaps the bulk of the trailing update on the side
+    // stream.  Panel buffers alternate so the two streams never share one.
+    bool bulk_recorded = false;  // lev[1] recorded by this sequence (never wait on an older record)
+    for (int i = nexist; i < nblk; i++) {
+        const int p0 = starts[i], p1 = blk_end(i);
+        const int p2 = (i + 1 < nblk) ? blk_end(i + 1) : n;
+        cd* vb = c.vbuf + (size_t)((i - nexist) & 1) * LDL_NB * c.ld;
+        k_ldl_diag<<<1, 256, 0, c.stream>>>(c.H, c.ld, p0, p1, c.dw, c.invD, c.status);
+        c.launches++;
+        if (p1 >= n) break;
+        k_ldl_trsm<<<(n - p1 + TRSM_COLS - 1) / TRSM_COLS, 256, sm1, c.stream>>>(c.H, c.ld, p0, p1, p1, n, c.invD, vb);
+        c.launches++;
+        cudaEventRecord(c.lev[0], c.stream);
+        // rows of the next panel wait for the previous panel's bulk update
+        if (bulk_recorded) cudaStreamWaitEvent(c.stream, c.lev[1], 0);
+        launch_update(c, c.stream, vb, p0, p1, p1, p2, p1, n);
+        // bulk: rows beyond the next panel
+        cudaStreamWaitEvent(c.side, c.lev[0], 0);
+        launch_update(c, c.side, vb, p0, p1, p2, n, p2, n);
+        cudaEventRecord(c.lev[1], c.side);
+        bulk_recorded = true;
+    }
+    if (bulk_recorded) cudaStreamWaitEvent(c.stream, c.lev[1], 0);
+    if (nblk > nexist) {
+        k_ldl_linv<<<nblk - nexist, 256, 2 * sm1, c.stream>>>(c.H, c.ld, c.dblk, nexist, c.linv);
         c.launches++;
     }
-    if (cudaGetLastError() != cudaSuccess) return -2;
-    c.blk_start = starts;
-    c.fact_n = n;
-    // panel boundaries for the cooperative solves (starts..., n)
-    std::vector<int> bounds(starts);
-    bounds.push_back(n);
-    if (cudaMemcpyAsync(c.dblk, bounds.data(), bounds.size() * sizeof(int), cudaMemcpyHostToDevice, c.stream) !=
+}
+
+// Factorise rows m0..n-1 of M = H - lambda~ S given the factor of rows
+// 0..m0-1.  The launch sequence depends only on (m0, n) and the existing
+// panel boundaries, so it is captured once into a CUDA graph (both streams)
+// and replayed.
+int ldlh_factor(Ctx& c, int m0, int n)
+{
+    if (m0 < 0 || m0 > n || n > c.ld) return -1;
+    if (m0 > c.fact_n) return -1;
+    const size_t sm1 = LDL_NB * DG_LD * sizeof(double2);
+    if (!g_ldl_attr) {
+        cudaFuncSetAttribute(k_ldl_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+        cudaFuncSetAttribute(k_ldl_linv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * sm1));
+        cudaFuncSetAttribute(k_ldl_update<64, 2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UPD_SMEM);
+        cudaFuncSetAttribute(k_ldl_update<16, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UPD_SMEM);
+        g_ldl_attr = true;
+    }
+    // block list: existing blocks truncated at m0, then new 64-row blocks
+    std::vector<int> starts;
+    for (int s : c.blk_start)
+        if (s < m0) starts.push_back(s);
+    const int nexist = (int)starts.size();
+    for (int s = m0; s < n; s += LDL_NB) starts.push_back(s);
+    // panel boundaries (starts..., n) for the inverse blocks and the solves
+    const int nb = (int)starts.size();
+    for (int i = 0; i < nb; i++) c.bounds_h[i] = starts[i];
+    c.bounds_h[nb] = n;
+    if (cudaMemcpyAsync(c.dblk, c.bounds_h, (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, c.stream) !=
         cudaSuccess)
         return -2;
+    std::vector<int> key = {m0, n};
+    key.insert(key.end(), starts.begin(), starts.begin() + nexist);
+    Ctx::LdlGraph* g = nullptr;
+    for (auto& e : c.ldl_graphs)
+        if (e.key == key) g = &e;
+    if (!g) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        bool ok = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            const long long l0 = c.launches;
+            enqueue_factor(c, m0, n, starts, nexist);
+            c.graph_launches = c.launches - l0;
+            c.launches = l0;
+            ok = cudaStreamEndCapture(c.stream, &graph) == cudaSuccess && graph &&
+                 cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+        }
+        if (graph) cudaGraphDestroy(graph);
+        if (!ok) {
+            cudaGetLastError();
+            if (exec) cudaGraphExecDestroy(exec);
+            // capture unavailable: run the launches directly
+            enqueue_factor(c, m0, n, starts, nexist);
+            if (cudaGetLastError() != cudaSuccess) return -2;
+            c.blk_start = starts;
+            c.fact_n = n;
+            return 0;
+        }
+        if (c.ldl_graphs.size() >= 8) {
+            cudaGraphExecDestroy(c.ldl_graphs.front().exec);
+            c.ldl_graphs.erase(c.ldl_graphs.begin());
+        }
+        c.ldl_graphs.push_back({key, exec});
+        g = &c.ldl_graphs.back();
+        g->launches = c.graph_launches;
+    }
+    if (cudaGraphLaunch(g->exec, c.stream) != cudaSuccess) return -2;
+    c.launches += g->launches;
+    c.blk_start = starts;
+    c.fact_n = n;
     return 0;
 }
 
