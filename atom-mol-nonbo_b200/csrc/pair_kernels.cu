@@ -16,6 +16,7 @@
 // Grid shape: one CTA per 32 x 32 tile of the lower triangle; lanes run
 // along the row index k (the contiguous index of the column-major H and S),
 // warps along the column index l.
+#include <string.h>
 #include "ecg_internal.h"
 #include "ecg_grad.cuh"
 
@@ -782,3 +783,148 @@ int launch_term_batch(Ctx& c, int count, const double* pk, const double* pl, con
 }
 
 }  // namespace ecg
+
+// ---------------------------------------------------------------------------
+// Adjoint gradient without any device allocation (ecg_adjoint_gradient_noalloc).
+//
+// Some hosts cannot allocate device memory at the point where they need the
+// gradient: an application that owns all GPU memory through its own pool and
+// forbids stray allocations, an optimiser callback that must not fail or
+// fragment memory in the middle of a long run, or a service with fixed
+// per-tenant memory budgets.  This variant takes every input and output as a
+// caller-owned device pointer and keeps all of its working data (per-function
+// bra/ket matrices, the projector terms and the per-tile partial sums) in one
+// fixed array compiled into the library.  Limits: at most NOALLOC_KMAX basis
+// functions and NOALLOC_TMAX projector terms; every GPU that loads the
+// library holds the array (about 4.3 MB) until the process exits.  All calls
+// on a device share the array, so calls whose GPU work overlaps (different
+// streams, other host threads) race on it; each call rewrites every part of
+// it that the call reads, so nothing has to start at zero.
+// ---------------------------------------------------------------------------
+#include <mutex>
+#include "../../include/ecg_abi.h"
+
+namespace ecg {
+namespace noalloc {
+
+constexpr int KMAX = 512;
+constexpr int TMAXN = 16;
+constexpr int NPMAX = 15;                  // n(n+1)/2 at n = 5
+constexpr int NVMAX = 2 * NPMAX + 1;
+constexpr long long TILES = (long long)(KMAX / TILE) * (KMAX / TILE + 1) / 2;
+
+constexpr size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+constexpr size_t OFF_P = 0;
+constexpr size_t OFF_COEF = OFF_P + align256(sizeof(double) * TMAXN * NMAX * NMAX);
+constexpr size_t OFF_BRA = OFF_COEF + align256(sizeof(double) * TMAXN);
+constexpr size_t OFF_KET = OFF_BRA + align256(sizeof(cd) * KMAX * NPMAX);
+constexpr size_t OFF_DET = OFF_KET + align256(sizeof(cd) * KMAX * TMAXN * NPMAX);
+constexpr size_t OFF_PART = OFF_DET + align256(sizeof(double) * KMAX);
+constexpr size_t BYTES = OFF_PART + align256(sizeof(double) * TILES * 2 * TILE * NVMAX);
+
+// The one scratch array.  Host code must not take its address directly (on
+// the host the name denotes a stand-in, not device memory); device_base()
+// obtains the device address with cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_scratch[BYTES];
+
+constexpr int MAX_DEVICES = 64;
+static std::mutex g_mu;
+static unsigned char* g_base[MAX_DEVICES] = {};
+
+// Device address of g_scratch on the current device, looked up once per
+// device (the first call on a device does it; that first call should come
+// before any stream capture).
+static int device_base(unsigned char** out)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) {
+        cudaGetLastError();
+        return ECG_ENODEV;
+    }
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!g_base[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return ECG_ECUDA;
+        }
+        g_base[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_base[dev];
+    return ECG_OK;
+}
+
+template <int N>
+static int run(const SysParams& sp, unsigned char* base, const double* params, const cd* cvec, const double* diagS,
+               double E, int nfru, int nfa, double* grad, cudaStream_t st)
+{
+    constexpr int NV = AdjNV<N>::value;
+    double* Pd = reinterpret_cast<double*>(base + OFF_P);
+    double* coef = reinterpret_cast<double*>(base + OFF_COEF);
+    cd* bra = reinterpret_cast<cd*>(base + OFF_BRA);
+    cd* ket = reinterpret_cast<cd*>(base + OFF_KET);
+    double* detL = reinterpret_cast<double*>(base + OFF_DET);
+    double* part = reinterpret_cast<double*>(base + OFF_PART);
+    k_prep<N><<<(nfa + 127) / 128, 128, 0, st>>>(params, Pd, sp.T, nfa, bra, ket, detL);
+    const int Rlo = nfru / TILE, Rhi = (nfa + TILE - 1) / TILE;
+    const long long nt = tile_count(Rlo, Rhi);
+    const size_t smem = (size_t)8 * TILE * NV * sizeof(double);
+    if (cudaFuncSetAttribute(k_adjoint<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return ECG_ECUDA;
+    k_adjoint<N><<<(unsigned)nt, 256, smem, st>>>(sp, coef, Pd, bra, ket, detL, diagS, cvec, E, nfru, nfa, Rlo, part);
+    const int nf = nfa - nfru;
+    k_adjoint_final<N><<<(nf * 32 + 255) / 256, 256, 0, st>>>(part, params, nfru, nfa, Rlo, Rhi, grad);
+    return cudaGetLastError() == cudaSuccess ? ECG_OK : ECG_ECUDA;
+}
+
+}  // namespace noalloc
+}  // namespace ecg
+
+extern "C" int ecg_adjoint_gradient_noalloc(int n, const double* mass_matrix_host, const double* charges_host,
+                                            int nterms, const int* yhy_mats_host, const int* yhy_coeffs_host,
+                                            const double* params_dev, const double* c_dev, const double* diagS_dev,
+                                            double energy, int nfru, int nfa, double* grad_dev, void* stream)
+{
+    using namespace ecg;
+    if (n < 2 || n > NMAX || nterms < 1 || nfru < 0 || nfa <= nfru) return ECG_EARG;
+    if (!mass_matrix_host || !charges_host || !yhy_mats_host || !yhy_coeffs_host || !params_dev || !c_dev ||
+        !diagS_dev || !grad_dev)
+        return ECG_EARG;
+    if (nfa > noalloc::KMAX || nterms > noalloc::TMAXN) return ECG_ELIMIT;
+    unsigned char* base = nullptr;
+    const int rb = noalloc::device_base(&base);
+    if (rb != ECG_OK) return rb;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    SysParams sp;
+    memset(&sp, 0, sizeof(sp));
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) sp.M[i * NMAX + j] = mass_matrix_host[i + j * n];
+    sp.q0 = charges_host[0];
+    for (int i = 0; i < n; i++) sp.q[i] = charges_host[1 + i];
+    sp.two_r3n2 = pow(2.0, (3 * n) / 2.0);
+    sp.n = n;
+    sp.T = nterms;
+    // projector terms go into the scratch array (double, row-major P[t][i][j])
+    double P[noalloc::TMAXN * NMAX * NMAX];
+    double cf[noalloc::TMAXN];
+    for (int t = 0; t < nterms; t++) {
+        for (int i = 0; i < NMAX; i++)
+            for (int j = 0; j < NMAX; j++)
+                P[(t * NMAX + i) * NMAX + j] = (i < n && j < n) ? yhy_mats_host[(size_t)t * n * n + i + j * n] : 0.0;
+        cf[t] = yhy_coeffs_host[t];
+    }
+    if (cudaMemcpyAsync(base + noalloc::OFF_P, P, sizeof(double) * nterms * NMAX * NMAX, cudaMemcpyHostToDevice, st) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(base + noalloc::OFF_COEF, cf, sizeof(double) * nterms, cudaMemcpyHostToDevice, st) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        return ECG_ECUDA;
+    }
+    const cd* cv = reinterpret_cast<const cd*>(c_dev);
+    switch (n) {
+        case 2: return noalloc::run<2>(sp, base, params_dev, cv, diagS_dev, energy, nfru, nfa, grad_dev, st);
+        case 3: return noalloc::run<3>(sp, base, params_dev, cv, diagS_dev, energy, nfru, nfa, grad_dev, st);
+        case 4: return noalloc::run<4>(sp, base, params_dev, cv, diagS_dev, energy, nfru, nfa, grad_dev, st);
+        default: return noalloc::run<5>(sp, base, params_dev, cv, diagS_dev, energy, nfru, nfa, grad_dev, st);
+    }
+}

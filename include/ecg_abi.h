@@ -34,6 +34,7 @@ extern "C" {
 #define ECG_ECUDA (-2)      /* CUDA runtime error */
 #define ECG_ENOMEM (-3)     /* device allocation failed */
 #define ECG_ENODEV (-4)     /* no CUDA device */
+#define ECG_ELIMIT (-5)     /* size above a fixed capacity of the call */
 
 typedef struct ecg_ctx ecg_ctx;
 
@@ -129,6 +130,28 @@ int ecg_timer_start(ecg_ctx* ctx);
 int ecg_timer_stop(ecg_ctx* ctx, double* ms);
 /* Bytes this context has copied host->device and device->host so far. */
 int ecg_io_bytes(ecg_ctx* ctx, long long* h2d, long long* d2h);
+/* The fused adjoint gradient of ecg_energy_ib_adjoint, for callers that
+ * cannot allocate device memory when they need it (a host that manages all
+ * GPU memory through its own pool, an optimiser callback that must not fail
+ * or fragment memory mid-run, a service with fixed memory budgets).  No
+ * counterpart in the reference.  Every input and output is caller-owned:
+ * params_dev = Glob_NonlinParam (npt x nfa doubles), c_dev = the normalised
+ * eigenvector Glob_c (nfa complex), diagS_dev = Glob_diagS (nfa), energy =
+ * its eigenvalue, grad_dev receives npt*(nfa-nfru) doubles ordered as
+ * ecg_energy_ib's gradient.  The system arguments are those of
+ * ecg_ctx_create.  Work is queued on `stream` (a cudaStream_t, NULL for the
+ * default stream) and the call returns without waiting for it.
+ * Limits: nfa <= 512 and nterms <= 16, else ECG_ELIMIT and nothing runs.
+ * The call allocates nothing: its working data lives in one fixed array of
+ * about 4.3 MB compiled into the library, held by every GPU that loads it
+ * until the process exits.  The first call on a device looks up that
+ * array's device address (make that first call before any stream capture).
+ * All calls on a device share the array: calls whose GPU work overlaps race
+ * on it and must be serialised by the caller. */
+int ecg_adjoint_gradient_noalloc(int n, const double* mass_matrix_host, const double* charges_host, int nterms,
+                                 const int* yhy_mats_host, const int* yhy_coeffs_host, const double* params_dev,
+                                 const double* c_dev, const double* diagS_dev, double energy, int nfru, int nfa,
+                                 double* grad_dev, void* stream);
 /* Measured FP64 FMA throughput of the device (TFLOP/s, 2 flops per FMA):
  * a register-resident FMA loop over all SMs, timed with CUDA events. */
 int ecg_probe_fp64_peak(int device, double* tflops);
