@@ -69,6 +69,7 @@ void free_ctx(Ctx& c)
     for (auto& g : c.ldl_graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     c.ldl_graphs.clear();
+    cand_free(c.cand);
     if (c.bounds_h) cudaFreeHost(c.bounds_h);
     if (c.status_h) cudaFreeHost(c.status_h);
     if (c.red_h) cudaFreeHost(c.red_h);
@@ -489,6 +490,17 @@ int ecg_energy_ib_adjoint(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, 
     if (!ctx || !energy || !num_iter) return ECG_EARG;
     return energy_ib_common(ctx->c, nfru, nfa, mat_elem_needed, approx_energy, tol, max_iter, energy, grad_host,
                             num_iter, true);
+}
+
+int ecg_eval_candidates(ecg_ctx* ctx, int nbase, int count, const double* cand_host, double approx_energy,
+                        double tol, int max_iter, double* energies_host, int* errcodes_host, int* num_iter_host,
+                        double* rel_acc_host)
+{
+    if (!ctx) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.dev) != cudaSuccess) return ECG_ECUDA;
+    return eval_candidates(c, nbase, count, cand_host, approx_energy, tol, max_iter, energies_host, errcodes_host,
+                           num_iter_host, rel_acc_host);
 }
 
 int ecg_get_matrices(ecg_ctx* ctx, int n, double* H_host, double* S_host, int ld_host, double* diagS_host,

@@ -21,6 +21,60 @@ inline long long tile_count(int Rlo, int Rhi)
     return tri(Rhi) - tri(Rlo);
 }
 
+// Number of k_cand_row tile shapes the autotuner chooses from.
+constexpr int CAND_ROW_SHAPES = 5;
+// Columns (candidates) per work item of the batched triangular solves and
+// the padding unit of the candidate column blocks.
+constexpr int CAND_NC = 16;
+constexpr int CAND_PAD = 64;
+
+// Workspace of the batched candidate evaluation (allocated on first use).
+// Column blocks are ldv x ccap, column j = candidate j, rows = base
+// functions, then CAND_PAD spare columns that pad the active set; the
+// border (row nbase+1) entries are separate vectors.  Per-column arrays use
+// the stride ccap.
+struct CandWork {
+    int bcap = 0;            // candidate capacity (multiple of CAND_PAD)
+    int ccap = 0;            // physical columns: bcap + CAND_PAD spare columns (stride of the per-column arrays)
+    int ldv = 0;             // rows of the column blocks (ld rounded up to 64)
+    int* cmap = nullptr;     // slot -> physical column of the active candidates (ccap)
+    double* par = nullptr;   // npt x bcap candidate parameters
+    cd* bra = nullptr;       // bcap x NP
+    cd* ket = nullptr;       // bcap x T x NP
+    double* det = nullptr;   // bcap
+    double* dS = nullptr;    // diagS of the candidate (its Re S_KK)
+    double* mu = nullptr;    // M(K, K) = Re H_KK / diagS - lambda~
+    cd* Mcol = nullptr;      // M(q, K), the bordered column of H - lambda~ S
+    cd* Scol = nullptr;      // S(q, K)
+    cd* Acol = nullptr;      // L0^-1 Mcol (unscaled new row of the factor)
+    cd* Lcol = nullptr;      // U(q, K) = invD o Acol (column K of L^H)
+    cd* V = nullptr;         // iterate v (rows < nbase)
+    cd* W = nullptr;         // B v
+    cd* Y = nullptr;         // forward solve
+    cd* Z = nullptr;         // invD o Y
+    cd* X = nullptr;         // backward solve (new x); Rayleigh products
+    cd* X2 = nullptr;        // second Rayleigh product
+    cd* brd = nullptr;       // border entries: [0] vK [1] wK [2] invDK [3] xK
+    double* nd = nullptr;    // NormOfDiff, NormOfDiffPrev, t1, t2, E
+    int* st = nullptr;       // active, iterations, ErrorCode, then the active count
+    int* st_h = nullptr;     // pinned host mirror of st
+    double* nd_h = nullptr;  // pinned host mirror of nd
+    unsigned* flags = nullptr;  // work-item flags of the cooperative solves
+    int nflags = 0;
+    int* bstart = nullptr;   // device panel boundaries of the base factor
+    int* bstart_h = nullptr; // pinned staging
+    int* abort_word = nullptr;
+    int solve_grid = 0;      // co-resident CTAs of the solve kernel
+    int row_variant = -1;    // autotuned k_cand_row shape
+    int tuned_n = 0, tuned_T = 0;
+    struct IterGraph {
+        std::vector<int> key;
+        cudaGraphExec_t exec = nullptr;
+        long long launches = 0;
+    };
+    std::vector<IterGraph> graphs;
+};
+
 struct Ctx {
     int dev = 0;
     int n = 0, np = 0, npt = 0, T = 0;
@@ -93,6 +147,8 @@ struct Ctx {
     cudaEvent_t ev[16];
     double stage_ms[8] = {0};
     int last_numiter = 0;
+
+    CandWork cand;           // batched candidate evaluation
 };
 
 enum StatusWord {
@@ -120,6 +176,13 @@ int launch_adjoint(Ctx& c, int nfru, int nfa, double E);
 int launch_plain_contract(Ctx& c, int nfo, int nfa, int nfru, double E);
 int launch_term_batch(Ctx& c, int count, const double* pk, const double* pl, const int* term, int gradflag,
                       cd* hs, cd* dk, cd* dl);
+
+int launch_cand_rows(Ctx& c, CandWork& cw, int nbase, int count, double approx_e, int variant);
+
+// ---- batched candidates (cand.cu) ----
+int eval_candidates(Ctx& c, int nbase, int count, const double* cand_host, double approx_e, double tol,
+                    int max_iter, double* energies, int* errcodes, int* num_iter, double* rel_acc);
+void cand_free(CandWork& cw);
 
 // ---- launchers (ldlh.cu) ----
 int ldlh_factor(Ctx& c, int m0, int n);

@@ -16,7 +16,9 @@
 //                 (the Hermitian rank-64 trailing update, a complex GEMM);
 //   k_ldl_linv    after the last panel: (U_pp^H)^-1 of every new panel.
 // The off-diagonal recurrence and the pivot d = conj(.) follow
-// src/linalg.f90:359-391 term for term; only the summation order differs.
+// src/linalg.f90:359-391 term for term; only the summation order differs,
+// and the pivots are kept real (the reference's complex arithmetic leaves a
+// rounding-level imaginary part in them).
 #include "ecg_internal.h"
 
 namespace ecg {
@@ -99,14 +101,15 @@ __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, in
                     for (int j = 0; j < 4; j++) rq[tx + 16 * j] = make_double2(w[i][j].x, w[i][j].y);
         }
         __syncthreads();
-        // pivot d = conj(dw_q), invD = 1/d (src/linalg.f90:375-383)
-        const double2 dq = rq[q];
-        const double nrm = dq.x * dq.x + dq.y * dq.y;
-        const double inrm = (nrm != 0.0) ? 1.0 / nrm : 0.0;
-        const cd iq = cd{dq.x * inrm, dq.y * inrm};  // 1 / conj(dw_q)
+        // pivot d = conj(dw_q), invD = 1/d (src/linalg.f90:375-383).  The
+        // pivots of a Hermitian matrix are real: the imaginary part of dw_q
+        // is rounding noise of the updates and is dropped (kept, it sets a
+        // floor of 1e-13..1e-12 under GHEPIIS's residual NormOfDiff).
+        const double dr = rq[q].x;
+        const cd iq = cd{(dr != 0.0) ? 1.0 / dr : 0.0, 0.0};
         if (tid == 0) {
             invD[p0 + q] = iq;
-            if (nrm == 0.0) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + q + 1);
+            if (dr == 0.0) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + q + 1);
         }
         cd wq[4];  // unscaled W(q, c) of this thread's columns
 #pragma unroll

@@ -645,6 +645,88 @@ __global__ void __launch_bounds__(128) k_term_batch(SysParams sp, const double* 
 }
 
 // ---------------------------------------------------------------------------
+// Candidate rows (the BasisEnlI trial loop, src/workproc.f90:4054-4070, where
+// each trial function becomes row nbase+1 of H and S).  Candidate j is the
+// bra, base function q the permuted ket, as for row k = nbase+1 of
+// ComputeMatElem (src/matform.f90:160-177); the StoreHS 'I' normalisation
+// (src/matform.f90:22-35) is applied and the row is kept as the upper column
+// it mirrors into: Mcol(q, j) = conj(M(K, q)), Scol(q, j) = conj(S(K, q)).
+// ---------------------------------------------------------------------------
+
+// Diagonal pair (K, K) of every candidate: diagS and M(K, K).
+template <int N>
+__global__ void __launch_bounds__(128) k_cand_diag(SysParams sp, const double* __restrict__ coef,
+                                                   const cd* __restrict__ cbra, const cd* __restrict__ cket,
+                                                   const double* __restrict__ cdet, int count, double approx_e,
+                                                   double* __restrict__ cdS, double* __restrict__ cmu)
+{
+    constexpr int NP = Sym<N>::NP;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    cd Ck[N][N];
+    load_sym<N>(cbra + (size_t)j * NP, Ck);
+    const double dj = cdet[j];
+    const double absdet = fabs(dj * dj);
+    cd Hs = mk(0.0, 0.0), Ss = mk(0.0, 0.0);
+    for (int t = 0; t < sp.T; t++) {
+        cd tCl[N][N];
+        load_sym<N>(cket + ((size_t)j * sp.T + t) * NP, tCl);
+        TermEnergy<N> te;
+        term_energy<N, false>(Ck, tCl, absdet, sp, te);
+        const double cf = coef[t];
+        Hs = rfma(cf, te.T + te.V, Hs);
+        Ss = rfma(cf, te.S, Ss);
+    }
+    cdS[j] = Ss.x;
+    cmu[j] = Hs.x / Ss.x - approx_e;
+}
+
+// Off-diagonal pairs (K, q), q < nbase, for all candidates.  Lanes run along
+// q (the contiguous index of the stored columns), the W warps of a CTA over
+// candidates, CPW candidates per warp.
+template <int N, int W, int CPW>
+__global__ void __launch_bounds__(W * 32) k_cand_row(SysParams sp, const double* __restrict__ coef,
+                                                     const cd* __restrict__ cbra, const double* __restrict__ cdet,
+                                                     const double* __restrict__ cdS, const cd* __restrict__ ket,
+                                                     const double* __restrict__ detL,
+                                                     const double* __restrict__ diagS, int nbase, int count,
+                                                     double approx_e, cd* __restrict__ Mcol, cd* __restrict__ Scol,
+                                                     int ldv)
+{
+    constexpr int NP = Sym<N>::NP;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int q = blockIdx.x * 32 + lane;
+    if (q >= nbase) return;
+    const double dq = detL[q];
+    const double dSq = diagS[q];
+#pragma unroll 1
+    for (int u = 0; u < CPW; u++) {
+        const int j = (blockIdx.y * W + w) * CPW + u;
+        if (j >= count) break;
+        cd Ck[N][N];
+        load_sym<N>(cbra + (size_t)j * NP, Ck);
+        const double absdet = fabs(dq * cdet[j]);
+        cd Hs = mk(0.0, 0.0), Ss = mk(0.0, 0.0);
+#pragma unroll 1
+        for (int t = 0; t < sp.T; t++) {
+            cd tCl[N][N];
+            load_sym<N>(ket + ((size_t)q * sp.T + t) * NP, tCl);
+            TermEnergy<N> te;
+            term_energy<N, false>(Ck, tCl, absdet, sp, te);
+            const double cf = __ldg(coef + t);
+            Hs = rfma(cf, te.T + te.V, Hs);
+            Ss = rfma(cf, te.S, Ss);
+        }
+        const double f = 1.0 / sqrt(cdS[j] * dSq);
+        const size_t o = (size_t)q + (size_t)j * ldv;
+        const cd s = f * Ss;
+        const cd m = f * (Hs - approx_e * Ss);
+        stcd(Scol + o, conj(s));
+        stcd(Mcol + o, conj(m));
+    }
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 #define ECG_DISPATCH_N(n, FN, ...)              \
@@ -780,6 +862,41 @@ int launch_term_batch(Ctx& c, int count, const double* pk, const double* pl, con
                       cd* dk, cd* dl)
 {
     ECG_DISPATCH_N(c.n, batch_n, c, count, pk, pl, term, gradflag, hs, dk, dl)
+}
+
+// Candidate rows.  variant = tile shape of k_cand_row (CAND_ROW_SHAPES):
+// warps per CTA x candidates per warp.
+template <int N, int W, int CPW>
+static void cand_row_launch(Ctx& c, CandWork& cw, int nbase, int count, double approx_e)
+{
+    dim3 g((nbase + 31) / 32, (count + W * CPW - 1) / (W * CPW));
+    k_cand_row<N, W, CPW><<<g, W * 32, 0, c.stream>>>(c.sp, c.coef, cw.bra, cw.det, cw.dS, c.ket, c.detL, c.diagS,
+                                                      nbase, count, approx_e, cw.Mcol, cw.Scol, cw.ldv);
+}
+
+template <int N>
+static int cand_rows_n(Ctx& c, CandWork& cw, int nbase, int count, double approx_e, int variant)
+{
+    if (count <= 0) return 0;
+    k_prep<N><<<(count + 127) / 128, 128, 0, c.stream>>>(cw.par, c.Pd, c.T, count, cw.bra, cw.ket, cw.det);
+    k_cand_diag<N><<<(count + 127) / 128, 128, 0, c.stream>>>(c.sp, c.coef, cw.bra, cw.ket, cw.det, count, approx_e,
+                                                              cw.dS, cw.mu);
+    c.launches += 2;
+    if (nbase > 0) {
+        switch (variant) {
+            case 0: cand_row_launch<N, 4, 1>(c, cw, nbase, count, approx_e); break;
+            case 1: cand_row_launch<N, 4, 2>(c, cw, nbase, count, approx_e); break;
+            case 2: cand_row_launch<N, 8, 1>(c, cw, nbase, count, approx_e); break;
+            case 3: cand_row_launch<N, 8, 2>(c, cw, nbase, count, approx_e); break;
+            default: cand_row_launch<N, 8, 4>(c, cw, nbase, count, approx_e); break;
+        }
+        c.launches++;
+    }
+    return last_err();
+}
+int launch_cand_rows(Ctx& c, CandWork& cw, int nbase, int count, double approx_e, int variant)
+{
+    ECG_DISPATCH_N(c.n, cand_rows_n, c, cw, nbase, count, approx_e, variant)
 }
 
 }  // namespace ecg

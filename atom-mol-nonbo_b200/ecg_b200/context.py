@@ -151,6 +151,25 @@ class Context:
         return self._energy_ib(self.lib.ecg_energy_ib_adjoint, "ecg_energy_ib_adjoint", nfru, nfa, approx_energy,
                                tol, max_iter, mat_elem_needed, want_grad)
 
+    def eval_candidates(self, nbase, candidates, approx_energy, tol, max_iter=20):
+        """The BasisEnlI trial loop (src/workproc.f90:4054-4070) for a batch:
+        for each row of `candidates` (count, npt), the energy of
+        EnergyIA(nbase+1, nbase+1) with that function as basis function
+        nbase+1.  Returns (E, ErrorCode, NumIter, RelAcc), one entry per
+        candidate; the context's basis is left unchanged."""
+        cand = np.ascontiguousarray(candidates, dtype=np.float64)
+        if cand.ndim != 2 or cand.shape[1] != self.npt:
+            raise ValueError(f"candidates must be (count, {self.npt})")
+        cnt = cand.shape[0]
+        E = np.zeros(cnt)
+        err = np.zeros(cnt, dtype=np.int32)
+        it = np.zeros(cnt, dtype=np.int32)
+        ra = np.zeros(cnt)
+        _check(self.lib.ecg_eval_candidates(self.h, int(nbase), cnt, dptr(cand), float(approx_energy), float(tol),
+                                            int(max_iter), dptr(E), iptr(err), iptr(it), dptr(ra)),
+               "ecg_eval_candidates")
+        return E, err, it, ra
+
     def matrix_elements(self, pk, pl, terms, gradflag=0):
         """MatrixElements for a batch: returns H, S (count,) and Dk, Dl
         (count, 4np) complex (None when not requested)."""

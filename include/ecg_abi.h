@@ -97,6 +97,31 @@ int ecg_energy_ib(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, double a
 int ecg_energy_ib_adjoint(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, double approx_energy, double tol,
                           int max_iter, double* energy, double* grad_host, int* num_iter);
 
+/* The trial loop of BasisEnlI (src/workproc.f90:4054-4070) for `count`
+ * candidate functions at once: for every candidate j, the energy that
+ *     Glob_NonlinParam(1:npt, nbase+1) = cand_host(1:npt, j)
+ *     E_j = EnergyIA(nbase+1, nbase+1, .true., ErrorCode_j)
+ * would return, i.e. ComputeMatElem(nbase+1, nbase+1) followed by
+ * GHEPIIS(nbase+1, nbase+1, ..., SpecifNorm -1) with the bordered LDL^H
+ * step of LDLHF (src/linalg.f90:316-391) for the new row.
+ * Requires: the context's H and S hold rows 1..nbase built with the same
+ * approx_energy (lambda~), as after EnergyIA(1, nbase); the LDL^H factor of
+ * those rows is reused when present, else computed first (ErrorCode 1 of
+ * that factorisation is returned as the call's status).
+ * Every candidate starts from Glob_LastEigvector(1:nbase+1) as the context
+ * holds it at the call (the sequential reference starts each trial from
+ * the previous trial's eigenvector; results agree to the tolerance).
+ * The context's own state (parameters, H, S, factor, vectors) is left as
+ * it was: install the chosen candidate with ecg_set_params and
+ * ecg_energy_ia(nbase+1, nbase+1, ...), as BasisEnlI does after its loop.
+ * Outputs per candidate: energies_host (undefined where the code is 1),
+ * errcodes_host (0, 1 = zero pivot in the new row, 2 = not converged in
+ * max_iter iterations), num_iter_host and rel_acc_host (NormOfDiff); the
+ * last three may be NULL.  Returns 0 or a negative ECG_E* status. */
+int ecg_eval_candidates(ecg_ctx* ctx, int nbase, int count, const double* cand_host, double approx_energy,
+                        double tol, int max_iter, double* energies_host, int* errcodes_host, int* num_iter_host,
+                        double* rel_acc_host);
+
 /* Device -> host copies of the context arrays (any pointer may be NULL).
  * H_host, S_host: n x n with leading dimension ld_host. */
 int ecg_get_matrices(ecg_ctx* ctx, int n, double* H_host, double* S_host, int ld_host, double* diagS_host,

@@ -156,3 +156,28 @@ class Oracle:
         g = np.zeros(nfo * self.npt)
         self.lib.orc_gradient_contract(nfo, nfa, nfru, _p(self.D), self.D.shape[1], _p(self.c), E, _p(g))
         return E, g, err, it
+
+    # BasisEnlI trial loop, src/workproc.f90:4054-4070
+    def trial_loop(self, nbase, candidates, approx_e, tol, start, max_iter=20):
+        """For each candidate: its parameters become function nbase+1 and
+        EnergyIA(nbase+1, nbase+1, .true.) runs (ComputeMatElem of row K,
+        then GHEPIIS(K, K) with the bordered LDLHF step).  Every trial starts
+        from `start` (Glob_LastEigvector(1:K)).  Requires H, S and the
+        LDL^H factor of the first nbase functions.  Returns arrays
+        (E, ErrorCode, NumIter, RelAcc)."""
+        K = nbase + 1
+        base = np.array(self.params[:nbase], dtype=np.float64)
+        cands = np.asarray(candidates, dtype=np.float64)
+        out = np.zeros(len(cands)), np.zeros(len(cands), dtype=np.int32), np.zeros(len(cands), dtype=np.int32), \
+            np.zeros(len(cands))
+        for j, cnd in enumerate(cands):
+            self.set_params(np.vstack([base, cnd[None, :]]))
+            self.compute_mat_elem(K, K, approx_e)
+            if K == 1:
+                out[0][j], out[1][j], out[2][j], out[3][j] = self.H[0, 0].real + approx_e, 0, 1, 0.0
+                continue
+            self.c[:K] = start[:K]
+            lam, ra, it, err = self.ghepiis(K, K, approx_e, tol, max_iter, -1)
+            out[0][j], out[1][j], out[2][j], out[3][j] = lam, err, it, ra
+        self.set_params(base)
+        return out
