@@ -340,7 +340,7 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
     r |= dalloc(&c.detL, L);
     r |= dalloc(&c.dw, L);
     r |= dalloc(&c.linv, L * LDL_NB);
-    r |= dalloc(&c.vbuf, 2 * L * LDL_NB);
+    r |= dalloc(&c.vbuf, 3 * L * LDL_NB);
     r |= dalloc(&c.status, (size_t)ST_COUNT);
     r |= dalloc(&c.red, (size_t)RD_COUNT);
     r |= dalloc(&c.counters, (size_t)4);

@@ -113,7 +113,7 @@ struct Ctx {
     // LDL^H workspace
     cd* dw = nullptr;           // working diagonal (ld)
     cd* linv = nullptr;         // ld x LDL_NB: inverse unit-lower diagonal blocks
-    cd* vbuf = nullptr;         // 2 x LDL_NB x ld: unscaled panel rows (ping-pong)
+    cd* vbuf = nullptr;         // 3 x LDL_NB x ld: unscaled panel rows (rotating)
     int* status = nullptr;      // device status words (see ST_*)
     int* status_h = nullptr;    // pinned host mirror
     double* red = nullptr;      // reduction scratch for the solver (doubles)

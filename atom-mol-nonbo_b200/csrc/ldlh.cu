@@ -60,93 +60,144 @@ __global__ void __launch_bounds__(256) k_ldl_mirror(cd* __restrict__ A, int ld, 
     }
 }
 
-// Diagonal block elimination.  The working 64 x 64 tile lives in
-// registers: thread (ty, tx) of a 16 x 16 layout owns rows ty + 16i and
-// columns tx + 16j (16 complex values, the working diagonal included).  At
-// step q the owners of row q publish it to a double-buffered shared row, one
-// barrier later every thread applies the rank-one update to its elements
-// (W(r,c) -= conj(U(q,r)) W(q,c), r < c; dw(c) -= conj(W(q,c)) U(q,c)), and
-// the row-q owners keep U(q,.) = invD_q W(q,.).
+// Diagonal block elimination, blocked by 8-row sub-panels.  The working
+// 64 x 64 upper triangle W(r, c), r <= c (diagonal from dw), sits in shared
+// memory.  Per sub-panel (rows s0..s0+7):
+//   (a) eight lanes of warp 0 eliminate the 8 x 8 diagonal sub-block in
+//       registers (lane j holds column j; pivots and row values by
+//       shuffle);
+//   (b) one thread per column c beyond the sub-block forms the unscaled
+//       rows Wun(q, c) = W(q, c) - sum_{q' < q} conj(U(q', q)) Wun(q', c)
+//       by substitution and U(q, c) = invD_q Wun(q, c);
+//   (c) all threads apply the rank-8 update W(r, c) -= sum_q conj(U(q, r))
+//       Wun(q, c) to the rows and columns beyond the sub-panel.
+// Three barriers per sub-panel.  The recurrence and the pivot
+// d = conj(W(q, q)) follow src/linalg.f90:359-391; pivots are real (the
+// imaginary part of W(q, q) is rounding noise of the updates and is
+// dropped: kept, it sets a floor of 1e-13..1e-12 under GHEPIIS's residual
+// NormOfDiff).
 constexpr int DG_LD = LDL_NB + 1;
+constexpr int DG_SUB = 8;
+constexpr size_t DG_SMEM = (size_t)(LDL_NB * DG_LD + DG_SUB * LDL_NB) * sizeof(double2);
+
 __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, int p0, int p1, cd* __restrict__ dw,
                                                    cd* __restrict__ invD, int* __restrict__ status)
 {
-    __shared__ double2 rowq[2][LDL_NB];
+    extern __shared__ double2 dsm[];
+    double2* Ws = dsm;                   // Ws[r * DG_LD + c], r <= c
+    double2* Wu = dsm + LDL_NB * DG_LD;  // Wu[q * LDL_NB + c]: unscaled rows of the sub-panel
+    __shared__ double sid[DG_SUB];       // invD of the sub-panel rows
     const int b = p1 - p0;
     const int tid = threadIdx.x;
-    const int ty = tid >> 4, tx = tid & 15;
-    cd w[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int r = ty + 16 * i, c = tx + 16 * j;
-            cd v = cd{0.0, 0.0};
-            if (r < b && c < b) {
-                if (r < c)
-                    v = A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld];
-                else if (r == c)
-                    v = dw[p0 + r];
+    for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
+        const int r = e & 63, c = e >> 6;
+        double2 v = make_double2(0.0, 0.0);
+        if (r < b && c < b) {
+            if (r < c) {
+                const cd a = A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld];
+                v = make_double2(a.x, a.y);
+            } else if (r == c) {
+                const cd a = dw[p0 + r];
+                v = make_double2(a.x, a.y);
             }
-            w[i][j] = v;
         }
-    for (int q = 0; q < b; q++) {
-        double2* rq = rowq[q & 1];
-        if ((q & 15) == ty) {
-            const int iq = q >> 4;
+        Ws[r * DG_LD + c] = v;
+    }
+    __syncthreads();
+    for (int s0 = 0; s0 < b; s0 += DG_SUB) {
+        const int nq = min(DG_SUB, b - s0);
+        // (a) 8 x 8 diagonal sub-block
+        if (tid < 32) {
+            const int j = tid & 7;  // lanes 8..31 shadow lanes 0..7 (same values, no stores)
+            cd col[DG_SUB];
 #pragma unroll
-            for (int i = 0; i < 4; i++)
-                if (i == iq)
+            for (int i = 0; i < DG_SUB; i++) {
+                const double2 v = (i <= j && j < nq) ? Ws[(s0 + i) * DG_LD + s0 + j] : make_double2(0.0, 0.0);
+                col[i] = cd{v.x, v.y};
+            }
 #pragma unroll
-                    for (int j = 0; j < 4; j++) rq[tx + 16 * j] = make_double2(w[i][j].x, w[i][j].y);
+            for (int q = 0; q < DG_SUB; q++) {
+                if (q < nq) {  // warp-uniform
+                    const double dr = __shfl_sync(0xffffffffu, col[q].x, q);  // Re W(q, q)
+                    const double id = (dr != 0.0) ? __drcp_rn(dr) : 0.0;
+                    if (tid == 0) {
+                        sid[q] = id;
+                        invD[p0 + s0 + q] = cd{id, 0.0};
+                        if (dr == 0.0) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + s0 + q + 1);
+                    }
+                    const cd wq = col[q];
+#pragma unroll
+                    for (int i = 1; i < DG_SUB; i++) {
+                        if (i > q) {
+                            cd w;  // W(q, i), held by lane i
+                            w.x = __shfl_sync(0xffffffffu, col[q].x, i);
+                            w.y = __shfl_sync(0xffffffffu, col[q].y, i);
+                            if (j >= i) col[i] = cfms(cd{w.x * id, -w.y * id}, wq, col[i]);
+                        }
+                    }
+                    if (j > q) col[q] = cd{wq.x * id, wq.y * id};
+                }
+            }
+            if (tid < 8) {
+#pragma unroll
+                for (int i = 0; i < DG_SUB; i++)
+                    if (i < j && j < nq) Ws[(s0 + i) * DG_LD + s0 + j] = make_double2(col[i].x, col[i].y);
+            }
         }
         __syncthreads();
-        // pivot d = conj(dw_q), invD = 1/d (src/linalg.f90:375-383).  The
-        // pivots of a Hermitian matrix are real: the imaginary part of dw_q
-        // is rounding noise of the updates and is dropped (kept, it sets a
-        // floor of 1e-13..1e-12 under GHEPIIS's residual NormOfDiff).
-        const double dr = rq[q].x;
-        const cd iq = cd{(dr != 0.0) ? 1.0 / dr : 0.0, 0.0};
-        if (tid == 0) {
-            invD[p0 + q] = iq;
-            if (dr == 0.0) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + q + 1);
-        }
-        cd wq[4];  // unscaled W(q, c) of this thread's columns
+        // (b) sub-panel rows beyond the sub-block, one thread per column
+        const int t0 = s0 + DG_SUB;
+        if (t0 < b && tid < b - t0) {
+            const int c = t0 + tid;
+            cd wun[DG_SUB];
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const double2 v = rq[tx + 16 * j];
-            wq[j] = cd{v.x, v.y};
-        }
+            for (int q = 0; q < DG_SUB; q++) {
+                if (q < nq) {
+                    const double2 w = Ws[(s0 + q) * DG_LD + c];
+                    cd v = cd{w.x, w.y};
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const int r = ty + 16 * i;
-            if (r > q && r < b) {
-                const double2 v = rq[r];
-                const cd cu = conj(cmul(cd{v.x, v.y}, iq));  // conj(U(q, r))
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const int c = tx + 16 * j;
-                    // W(r,c) -= conj(U(q,r)) W(q,c)
-                    if (c > r && c < b) w[i][j] = cfms(cu, wq[j], w[i][j]);
-                }
-                // diagonal (c == r iff tx == ty, j == i): dw -= conj(W(q,r)) U(q,r)
-                if (tx == ty) w[i][i] = cfms(cd{v.x, -v.y}, conj(cu), w[i][i]);
-            } else if (r == q) {
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const int c = tx + 16 * j;
-                    if (c > q && c < b) w[i][j] = cmul(wq[j], iq);  // U(q, c)
+                    for (int q2 = 0; q2 < q; q2++) {
+                        const double2 u = Ws[(s0 + q2) * DG_LD + s0 + q];  // U(q2, q)
+                        v = cfms(cd{u.x, -u.y}, wun[q2], v);
+                    }
+                    wun[q] = v;
+                    Wu[q * LDL_NB + c] = make_double2(v.x, v.y);
+                    const double id = sid[q];
+                    Ws[(s0 + q) * DG_LD + c] = make_double2(v.x * id, v.y * id);
+                } else {
+                    wun[q] = cd{0.0, 0.0};
                 }
             }
         }
-    }
+        __syncthreads();
+        // (c) rank-8 update of the rows and columns beyond the sub-panel
+        if (t0 < b) {
+            const int m = b - t0;
+            for (int e = tid; e < m * m; e += 256) {
+                const int r = t0 + e / m, c = t0 + e % m;
+                if (r > c) continue;
+                const double2 w = Ws[r * DG_LD + c];
+                cd acc = cd{w.x, w.y};
 #pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int r = ty + 16 * i, c = tx + 16 * j;
-            if (r < c && c < b) A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld] = w[i][j];
+                for (int q = 0; q < DG_SUB; q++) {
+                    if (q < nq) {
+                        const double2 u = Ws[(s0 + q) * DG_LD + r];  // U(q, r)
+                        const double2 v = Wu[q * LDL_NB + c];        // Wun(q, c)
+                        acc = cfms(cd{u.x, -u.y}, cd{v.x, v.y}, acc);
+                    }
+                }
+                Ws[r * DG_LD + c] = make_double2(acc.x, acc.y);
+            }
         }
+        __syncthreads();
+    }
+    for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
+        const int r = e & 63, c = e >> 6;
+        if (r < c && c < b) {
+            const double2 v = Ws[r * DG_LD + c];
+            A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld] = cd{v.x, v.y};
+        }
+    }
 }
 
 // Inverse of the unit lower diagonal block L_pp = U_pp^H of every panel in
@@ -280,7 +331,7 @@ __device__ __forceinline__ void mma_f64(double& c0, double& c1, double a, double
 }
 
 template <int TC, int WR, int WC>
-__global__ void __launch_bounds__(256) k_ldl_update(cd* __restrict__ A, int ld, int p0, int p1, int r0, int rend,
+__global__ void __launch_bounds__(256, 2) k_ldl_update(cd* __restrict__ A, int ld, int p0, int p1, int r0, int rend,
                                                      int c0, int n, const cd* __restrict__ vbuf, cd* __restrict__ dw)
 {
     constexpr int MT = LDL_NB / WR / 8;  // 8 x 8 tiles per warp along rows
@@ -304,6 +355,23 @@ __global__ void __launch_bounds__(256) k_ldl_update(cd* __restrict__ A, int ld, 
         for (int nt = 0; nt < NT; nt++)
 #pragma unroll
             for (int e = 0; e < 2; e++) accr[mt][nt][e] = acci[mt][nt][e] = 0.0;
+    // the tile's current values, loaded together up front so that their
+    // latency overlaps the products (stored back after them)
+    double2 old[MT][NT][2];
+#pragma unroll
+    for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+        for (int nt = 0; nt < NT; nt++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int r = rb + (wr * MT + mt) * 8 + g;
+                const int c = cb + (wc * NT + nt) * 8 + t4 * 2 + e;
+                double2 v = make_double2(0.0, 0.0);
+                if (r < rend && c < n && c >= r)
+                    v = (c == r) ? *reinterpret_cast<const double2*>(dw + c)
+                                 : *reinterpret_cast<const double2*>(A + (size_t)r + (size_t)c * ld);
+                old[mt][nt][e] = v;
+            }
     for (int k0 = 0; k0 < b; k0 += UPD_KC) {
         for (int e = tid; e < UPD_KC * LDL_NB; e += blockDim.x) {
             const int q = e % UPD_KC, mm = e / UPD_KC;
@@ -351,29 +419,22 @@ __global__ void __launch_bounds__(256) k_ldl_update(cd* __restrict__ A, int ld, 
         __syncthreads();
     }
 #pragma unroll
-    for (int mt = 0; mt < MT; mt++) {
-        const int r = rb + (wr * MT + mt) * 8 + g;
-        if (r >= rend) continue;
+    for (int mt = 0; mt < MT; mt++)
 #pragma unroll
         for (int nt = 0; nt < NT; nt++)
 #pragma unroll
             for (int e = 0; e < 2; e++) {
+                const int r = rb + (wr * MT + mt) * 8 + g;
                 const int c = cb + (wc * NT + nt) * 8 + t4 * 2 + e;
-                if (c >= n || c < r) continue;
+                if (r >= rend || c >= n || c < r) continue;
                 const double vr = accr[mt][nt][e], vi = acci[mt][nt][e];
-                if (c == r) {
-                    // dw -= conj(sum conj(U) Wun) = sum conj(Wun) U (src/linalg.f90:370-372)
-                    cd d = dw[c];
-                    d.x -= vr;
-                    d.y += vi;
-                    dw[c] = d;
-                } else {
-                    cd& a = A[(size_t)r + (size_t)c * ld];
-                    a.x -= vr;
-                    a.y -= vi;
-                }
+                const double2 o = old[mt][nt][e];
+                // diagonal: dw -= conj(sum conj(U) Wun) = sum conj(Wun) U (src/linalg.f90:370-372)
+                if (c == r)
+                    *reinterpret_cast<double2*>(dw + c) = make_double2(o.x - vr, o.y + vi);
+                else
+                    *reinterpret_cast<double2*>(A + (size_t)r + (size_t)c * ld) = make_double2(o.x - vr, o.y - vi);
             }
-    }
 }
 
 static bool g_ldl_attr = false;
@@ -417,31 +478,41 @@ static void enqueue_factor(Ctx& c, int m0, int n, const std::vector<int>& starts
         c.launches++;
         launch_update(c, c.stream, c.vbuf, p0, p1, p1, n, m0, n);
     }
-    // new panels, right-looking with a depth-one lookahead: the rows of the
-    // next panel are updated first on the main stream, so that panel's
-    // factorisation overlaps the bulk of the trailing update on the side
-    // stream.  Panel buffers alternate so the two streams never share one.
+    // new panels, right-looking with a lookahead: the rows of the next panel
+    // are updated first on the main stream, so that panel's factorisation
+    // overlaps the trailing update running on the side stream.  The
+    // trailing update of panel i is split: first the rows of panel i+2
+    // (after which lev[1] is recorded; the lookahead update of panel i+1
+    // needs only those), then the rest, which thus has two panel steps to
+    // complete before the lookahead of panel i+2 touches its rows.  Three
+    // panel buffers rotate, so a buffer is rewritten only after the update
+    // that reads it has finished (stream order through lev[1]).
     bool bulk_recorded = false;  // lev[1] recorded by this sequence (never wait on an older record)
     for (int i = nexist; i < nblk; i++) {
         const int p0 = starts[i], p1 = blk_end(i);
         const int p2 = (i + 1 < nblk) ? blk_end(i + 1) : n;
-        cd* vb = c.vbuf + (size_t)((i - nexist) & 1) * LDL_NB * c.ld;
-        k_ldl_diag<<<1, 256, 0, c.stream>>>(c.H, c.ld, p0, p1, c.dw, c.invD, c.status);
+        const int p3 = (i + 2 < nblk) ? blk_end(i + 2) : n;
+        cd* vb = c.vbuf + (size_t)((i - nexist) % 3) * LDL_NB * c.ld;
+        k_ldl_diag<<<1, 256, DG_SMEM, c.stream>>>(c.H, c.ld, p0, p1, c.dw, c.invD, c.status);
         c.launches++;
         if (p1 >= n) break;
         k_ldl_trsm<<<(n - p1 + TRSM_COLS - 1) / TRSM_COLS, 256, sm1, c.stream>>>(c.H, c.ld, p0, p1, p1, n, c.invD, vb);
         c.launches++;
         cudaEventRecord(c.lev[0], c.stream);
-        // rows of the next panel wait for the previous panel's bulk update
+        // rows of the next panel wait for the previous trailing update's first part
         if (bulk_recorded) cudaStreamWaitEvent(c.stream, c.lev[1], 0);
         launch_update(c, c.stream, vb, p0, p1, p1, p2, p1, n);
-        // bulk: rows beyond the next panel
         cudaStreamWaitEvent(c.side, c.lev[0], 0);
-        launch_update(c, c.side, vb, p0, p1, p2, n, p2, n);
+        launch_update(c, c.side, vb, p0, p1, p2, p3, p2, n);
         cudaEventRecord(c.lev[1], c.side);
+        launch_update(c, c.side, vb, p0, p1, p3, n, p3, n);
         bulk_recorded = true;
     }
-    if (bulk_recorded) cudaStreamWaitEvent(c.stream, c.lev[1], 0);
+    if (bulk_recorded) {
+        // join everything queued on the side stream
+        cudaEventRecord(c.lev[0], c.side);
+        cudaStreamWaitEvent(c.stream, c.lev[0], 0);
+    }
     if (nblk > nexist) {
         k_ldl_linv<<<nblk - nexist, 256, 2 * sm1, c.stream>>>(c.H, c.ld, c.dblk, nexist, c.linv);
         c.launches++;
@@ -459,6 +530,7 @@ int ldlh_factor(Ctx& c, int m0, int n)
     const size_t sm1 = LDL_NB * DG_LD * sizeof(double2);
     if (!g_ldl_attr) {
         cudaFuncSetAttribute(k_ldl_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+        cudaFuncSetAttribute(k_ldl_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DG_SMEM);
         cudaFuncSetAttribute(k_ldl_linv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * sm1));
         cudaFuncSetAttribute(k_ldl_update<64, 2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UPD_SMEM);
         cudaFuncSetAttribute(k_ldl_update<16, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UPD_SMEM);
