@@ -170,24 +170,48 @@ __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, in
             }
         }
         __syncthreads();
-        // (c) rank-8 update of the rows and columns beyond the sub-panel
+        // (c) rank-8 update of the rows and columns beyond the sub-panel:
+        // thread (rr, cc) owns rows t0 + rr + 16 i and columns t0 + cc + 16 j
         if (t0 < b) {
-            const int m = b - t0;
-            for (int e = tid; e < m * m; e += 256) {
-                const int r = t0 + e / m, c = t0 + e % m;
-                if (r > c) continue;
-                const double2 w = Ws[r * DG_LD + c];
-                cd acc = cd{w.x, w.y};
+            const int rr = tid >> 4, cc = tid & 15;
+            const int nblk = (b - t0 + 15) >> 4;  // 16-wide blocks of the trailing part
+            cd acc[4][4];
 #pragma unroll
-                for (int q = 0; q < DG_SUB; q++) {
-                    if (q < nq) {
-                        const double2 u = Ws[(s0 + q) * DG_LD + r];  // U(q, r)
-                        const double2 v = Wu[q * LDL_NB + c];        // Wun(q, c)
-                        acc = cfms(cd{u.x, -u.y}, cd{v.x, v.y}, acc);
-                    }
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int jj = 0; jj < 4; jj++) {
+                    const int r = t0 + rr + 16 * i, c = t0 + cc + 16 * jj;
+                    double2 w = make_double2(0.0, 0.0);
+                    if (r < b && c < b && r <= c) w = Ws[r * DG_LD + c];
+                    acc[i][jj] = cd{w.x, w.y};
                 }
-                Ws[r * DG_LD + c] = make_double2(acc.x, acc.y);
+#pragma unroll
+            for (int q = 0; q < DG_SUB; q++) {
+                if (q < nq) {
+                    cd u[4], v[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const int r = t0 + rr + 16 * i;
+                        const double2 x = (r < b) ? Ws[(s0 + q) * DG_LD + r] : make_double2(0.0, 0.0);  // U(q, r)
+                        u[i] = cd{x.x, -x.y};
+                        const int c = t0 + cc + 16 * i;
+                        const double2 y = (c < b) ? Wu[q * LDL_NB + c] : make_double2(0.0, 0.0);  // Wun(q, c)
+                        v[i] = cd{y.x, y.y};
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+#pragma unroll
+                        for (int jj = 0; jj < 4; jj++)
+                            if (i <= jj && jj < nblk) acc[i][jj] = cfms(u[i], v[jj], acc[i][jj]);  // block-uniform
+                }
             }
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int jj = 0; jj < 4; jj++) {
+                    const int r = t0 + rr + 16 * i, c = t0 + cc + 16 * jj;
+                    if (r < b && c < b && r <= c) Ws[r * DG_LD + c] = make_double2(acc[i][jj].x, acc[i][jj].y);
+                }
         }
         __syncthreads();
     }
