@@ -43,6 +43,7 @@ PROTOTYPES = {
     "ecg_timer_stop": (C.c_int, [_vp, _dp]),
     "ecg_io_bytes": (C.c_int, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "ecg_probe_fp64_peak": (C.c_int, [C.c_int, _dp]),
+    "ecg_probe_fp64_tensor_peak": (C.c_int, [C.c_int, _dp]),
     "ecg_adjoint_gradient_noalloc": (C.c_int, [C.c_int, _dp, _dp, C.c_int, _ip, _ip, C.c_void_p, C.c_void_p,
                                                C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
 }

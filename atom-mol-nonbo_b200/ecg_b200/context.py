@@ -13,7 +13,7 @@ import numpy as np
 from . import _lib
 from ._lib import dptr, iptr
 
-__all__ = ["Context", "EcgError", "probe_fp64_peak"]
+__all__ = ["Context", "EcgError", "probe_fp64_peak", "probe_fp64_tensor_peak"]
 
 
 class EcgError(RuntimeError):
@@ -221,4 +221,12 @@ def probe_fp64_peak(device=0):
     lib = _lib.load()
     t = C.c_double()
     _check(lib.ecg_probe_fp64_peak(int(device), C.byref(t)), "ecg_probe_fp64_peak")
+    return t.value
+
+
+def probe_fp64_tensor_peak(device=0):
+    """Measured FP64 tensor-core (mma.sync f64) throughput in TFLOP/s."""
+    lib = _lib.load()
+    t = C.c_double()
+    _check(lib.ecg_probe_fp64_tensor_peak(int(device), C.byref(t)), "ecg_probe_fp64_tensor_peak")
     return t.value

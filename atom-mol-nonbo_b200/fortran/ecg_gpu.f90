@@ -8,6 +8,7 @@
 !   GHEPIIS(k,n,...)                   -> GPU_GHEPIIS(k,n,apprlambda,Tol,lambda,RelAcc,MaxIter,SpecifNorm,NumIter,ErrorCode)
 !   EnergyIA / EnergyIAM               -> GPU_EnergyIA(Nmin,Nmax,AreMatElemNeeded,SpecifNorm,ErrorCode)
 !   EnergyIB                           -> GPU_EnergyIB(Evalue,Gradient,AreMatElemNeeded,ErrorCode)
+!   BasisEnlI trial loop (Kstep = 1)   -> GPU_EvalTrials(nfru,NTrials,ParSets,Energies,ErrorCodes)
 !
 !The Glob_* matrices live on the GPU inside the context; GPU_GetMatrices
 !copies Glob_H/Glob_S/Glob_diagS/Glob_invD back where host code (pruning,
@@ -81,6 +82,16 @@ interface
     real(c_double), intent(out) :: energy
     real(c_double), intent(out) :: grad(*)
     integer(c_int), intent(out) :: num_iter
+  end function
+  integer(c_int) function ecg_eval_candidates(ctx, nbase, count, cand, approx_energy, tol, max_iter, energies, &
+      errcodes, num_iter, rel_acc) bind(C, name='ecg_eval_candidates')
+    import :: c_int, c_double, c_ptr
+    type(c_ptr), value :: ctx
+    integer(c_int), value :: nbase, count, max_iter
+    real(c_double), intent(in) :: cand(*)
+    real(c_double), value :: approx_energy, tol
+    real(c_double), intent(out) :: energies(*), rel_acc(*)
+    integer(c_int), intent(out) :: errcodes(*), num_iter(*)
   end function
   integer(c_int) function ecg_get_matrices(ctx, n, H, S, ld, diagS, diagH, invD) bind(C, name='ecg_get_matrices')
     import :: c_int, c_double, c_ptr, c_double_complex
@@ -171,6 +182,29 @@ subroutine GPU_EnergyIB(Evalue, Gradient, AreMatElemNeeded, ErrorCode)
   Glob_InvItTempCounter1 = Glob_InvItTempCounter1 + 1
   Glob_InvItTempCounter2 = Glob_InvItTempCounter2 + it
 end subroutine GPU_EnergyIB
+
+!The trial loop of BasisEnlI (src/workproc.f90:4054-4070) with Kstep = 1,
+!all trials in one call: ParSets(1:npt,i) are the NTrials candidates drawn
+!by GenerateTrialParam beforehand; Energies(i) and ErrorCodes(i) are what
+!EnergyIA(nfru+1,nfru+1,.true.,ErrorCode) returns for candidate i.  The
+!basis of nfru functions must be current on the device (as after the
+!EnergyIA(1,nfru) that precedes the loop); it is left unchanged, so the
+!chosen candidate is installed afterwards with GPU_EnergyIA(nfru+1,nfru+1,...)
+!exactly as the reference does after its loop.
+subroutine GPU_EvalTrials(nfru, NTrials, ParSets, Energies, ErrorCodes)
+  integer, intent(in) :: nfru, NTrials
+  real(dprec), intent(in) :: ParSets(Glob_npt, NTrials)
+  real(dprec), intent(out) :: Energies(NTrials)
+  integer, intent(out) :: ErrorCodes(NTrials)
+  integer(c_int) :: st, codes(NTrials), iters(NTrials)
+  real(c_double) :: relacc(NTrials)
+  st = ecg_eval_candidates(ecg_ctx, nfru, NTrials, ParSets, Glob_ApproxEnergy, Glob_EigvalTol, &
+                           Glob_MaxIterForGHEPIIS, Energies, codes, iters, relacc)
+  if (st /= 0) stop 'GPU_EvalTrials: ecg_eval_candidates failed'
+  ErrorCodes = codes
+  Glob_InvItTempCounter1 = Glob_InvItTempCounter1 + NTrials
+  Glob_InvItTempCounter2 = Glob_InvItTempCounter2 + sum(iters)
+end subroutine GPU_EvalTrials
 
 !Copy the device matrices and vectors back into the Glob_* host arrays for
 !code that still reads them on the host.

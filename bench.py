@@ -39,7 +39,7 @@ CONFIG_INDEX = 2
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--K", type=int, default=None, help="override the basis size (testing only)")
@@ -48,6 +48,8 @@ def parse():
                          "decreasing, once below |tol| (src/linalg.f90:1900-1906)")
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--cpu-baseline", type=int, default=1)
+    ap.add_argument("--candidates", type=int, default=1, help="also time the batched-candidate configuration")
+    ap.add_argument("--cand-K", type=int, default=2000)
     ap.add_argument("--lam", type=float, default=None,
                     help="use this lambda~ instead of searching for one (profiling runs)")
     return ap.parse_args()
@@ -111,7 +113,7 @@ class ClockSampler:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh,
                                          stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -178,7 +180,7 @@ def flush_l2(buf):
 def run_ours(args, dist):
     import torch
 
-    from ecg_b200 import Context, probe_fp64_peak
+    from ecg_b200 import Context, probe_fp64_peak, probe_fp64_tensor_peak
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import opcount
 
@@ -268,36 +270,47 @@ def run_ours(args, dist):
                  "stages_ms": dict(zip(["pairs_hs_and_derivs", "ldlh", "invit", "contract"],
                                        (pstage / args.plain_steps).round(4).tolist()))}
 
-    # ---- roofline of the dominant kernel --------------------------------
+    # ---- rooflines: every stage, the dominant one as `roofline` -----------
     st = stage / args.steps
     names = ["pairs_hs", "ldlh", "invit", "adjoint"]
-    peak = probe_fp64_peak(dev)
+    peak_fma = probe_fp64_peak(dev)
+    peak_tc = probe_fp64_tensor_peak(dev)
     counts = opcount.pair_counts(sysm.n, T)
     adj_flop = counts["adjoint"]["total"] * pairs
     hs_flop = counts["reference_energy"]["total"] * pairs
     ldl_flop = 4.0 / 3.0 * K ** 3
-    per_stage_tf = {"pairs_hs": hs_flop / (st[0] * 1e-3) / 1e12, "ldlh": ldl_flop / (st[1] * 1e-3) / 1e12,
-                    "adjoint": adj_flop / (st[3] * 1e-3) / 1e12}
-    dom = int(np.argmax(st))
-    dom_name = names[dom]
-    traffic = None
+    invit_bytes = 32.0 * K * K * max(np.mean(iters), 1) + 32.0 * K * K  # iterations + the Rayleigh quotient
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0, "fallback": True}
+    traffic = {}
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(dom_name)
-    if dom_name in per_stage_tf:
-        achieved = per_stage_tf[dom_name]
-        roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": dom_name,
-                "peak_source": "measured in this run: register FMA loop over all SMs (no FP64 entry in "
-                               "MEASURED_PEAKS.json)"}
-    else:
-        # solver-dominated: the triangular solves are HBM/latency bound
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
-        bytes_it = 32.0 * K * K
-        achieved = bytes_it * max(np.mean(iters), 1) / (st[2] * 1e-3) / 1e9
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "kernel": dom_name}
+        traffic = json.load(open(tpath))
+    fma_src = "measured in this run: register FMA loop over all SMs (MEASURED_PEAKS.json has no FP64 entry)"
+    tc_src = ("measured in this run: register mma.sync.m8n8k4.f64 loop over all SMs "
+              "(MEASURED_PEAKS.json has no FP64 entry)")
+    hbm_src = "MEASURED_PEAKS.json hbm_gbs" + (" (fallback)" if peaks.get("fallback") else "")
+
+    def roof(bound, work, ms, peak, unit, kern, src, tkey):
+        ach = work / (ms * 1e-3) / (1e12 if unit == "TFLOP/s" else 1e9)
+        return {"bound": bound, "achieved": ach, "peak": peak, "unit": unit, "frac": ach / peak,
+                "traffic": traffic.get(tkey), "kernel": kern, "peak_source": src,
+                "algorithmic": work, "algorithmic_unit": "flop" if unit == "TFLOP/s" else "byte"}
+
+    stage_roof = {
+        "pairs_hs": roof("fp64", hs_flop, st[0], peak_fma, "TFLOP/s",
+                         "k_pair_energy<3> (+ k_pair_diag, k_prep): one launch per step", fma_src, "pairs_hs"),
+        "ldlh": roof("tensor", ldl_flop, st[1], peak_tc, "TFLOP/s",
+                     "LDL^H factorisation, one CUDA-graph launch per step: k_ldl_update trailing updates on the "
+                     "FP64 tensor cores, k_ldl_diag / k_ldl_trsm panel kernels", tc_src, "ldlh"),
+        "invit": roof("hbm", invit_bytes, st[2], peaks["hbm_gbs"], "GB/s",
+                      "inverse iterations (k_hemv, k_fwd_coop, k_bwd_coop) + Rayleigh quotient", hbm_src, "invit"),
+        "adjoint": roof("fp64", adj_flop, st[3], peak_fma, "TFLOP/s",
+                        "k_adjoint<3> + k_adjoint_final<3>: one launch each per step", fma_src, "adjoint"),
+    }
+    dom_name = names[int(np.argmax(st))]
+    roof_line = dict(stage_roof[dom_name])
+    per_stage_tf = {k: round(v["achieved"], 3) for k, v in stage_roof.items() if v["unit"] == "TFLOP/s"}
 
     line = {
         "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": dist.world, "steps": args.steps,
@@ -311,18 +324,21 @@ def run_ours(args, dist):
         "pairs_per_s": pairs * value, "pair_terms_per_s": pairs * T * value,
         "energy": E, "invit_iters": float(np.mean(iters)),
         "stages_ms": dict(zip(names, st.round(4).tolist())),
-        "stage_tflops": {k: round(v, 3) for k, v in per_stage_tf.items()},
+        "stage_tflops": per_stage_tf,
+        "stage_rooflines": stage_roof,
         "plain_gpu": plain,
         "adjoint_speedup_vs_plain": (value / plain["value"]) if plain else None,
         "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": (h1 - h0) // args.steps,
                 "d2h_bytes_per_step": (d1 - d0) // args.steps},
         "gpu_launches": int(launches),
-        "roofline": roof,
+        "roofline": roof_line,
         "clocks": clk,
     }
     if args.cpu_baseline and dist.rank == 0:
         line["cpu_baseline"] = cpu_sample(sysm, params, lam, K, budget_s=20.0, iters=np.mean(iters))
     ctx.close()
+    if args.candidates:
+        line["candidates"] = run_candidates(args, dev, dist.rank, cpu=bool(args.cpu_baseline and dist.rank == 0))
     return line
 
 
@@ -378,6 +394,88 @@ def cpu_sample(sysm, params, lam, K, budget_s=20.0, iters=3.0):
             "seconds_per_eval": t_eval,
             "parts_s": {"pairs": t_pairs, "ldlhf": t_ldl * scale3, "invit": t_it * iters * scale2},
             "cpu": platform.processor() or platform.machine()}
+
+
+def run_candidates(args, dev, rank, cpu=True):
+    """The batched configuration: the BasisEnlI trial loop with K = 2000
+    existing functions (seed 1003) and 256 candidates per call, drawn by
+    GenerateTrialParam's rule (synth.candidates).  Times ecg_eval_candidates
+    (all candidates in one call) against one candidate per call
+    (ecg_set_params + ecg_energy_ia(K+1, K+1), the reference's sequence),
+    both with host buffers, plus the oracle's trial loop on a bounded sample."""
+    from ecg_b200 import Context, synth
+    cfg = synth.CONFIGS[3]
+    K0, B = args.cand_K, cfg["candidates"]
+    sysm, params = synth.config_basis(3, K=K0)
+    if rank:
+        params = synth.random_basis(sysm.n, K0, cfg["seed"] + 7919 * rank)
+    cands = synth.candidates(params, B, cfg["seed"])
+    e_floor = synth.SYSTEMS[cfg["system"]]["e_floor"]
+    with Context(sysm, K0 + 1, device=dev) as ctx:
+        ctx.set_params(params)
+        ctx.set_vectors(K0, last_eigvec=np.ones(K0, dtype=np.complex128))
+        E0, _, _ = ctx.energy_ia(1, K0, e_floor, -1e-12, max_iter=200)
+        lam = E0 * INVIT_PARAMETER
+        ctx.set_vectors(K0, last_eigvec=np.ones(K0, dtype=np.complex128))
+        Eb, errb, _ = ctx.energy_ia(1, K0, lam, 1e-12)
+        _, x = ctx.vectors(K0 + 1)
+        start = x.copy()
+        start[K0] = 0.0
+        launches0 = ctx.launch_count()
+        for _ in range(max(1, args.warmup // 2)):
+            ctx.set_vectors(K0 + 1, last_eigvec=start)
+            ctx.eval_candidates(K0, cands, lam, 1e-12)
+        ms, nrep = 0.0, 3
+        for _ in range(nrep):
+            ctx.set_vectors(K0 + 1, last_eigvec=start)
+            ctx.timer_start()
+            E, err, it, _ = ctx.eval_candidates(K0, cands, lam, 1e-12)
+            ms += ctx.timer_stop()
+        ms /= nrep
+        n1, ms1 = 16, 0.0
+        single = []
+        for j in range(n1):
+            ctx.set_params(cands[j:j + 1], first=K0 + 1)
+            ctx.set_vectors(K0 + 1, last_eigvec=start)
+            ctx.timer_start()
+            Ej, ej, _ = ctx.energy_ia(K0 + 1, K0 + 1, lam, 1e-12)
+            ms1 += ctx.timer_stop()
+            single.append(abs(Ej - E[j]) if (ej == 0 and err[j] == 0) else 0.0)
+    out = {"workload": f"BasisEnlI trial loop n=3 K={K0} + {B} candidates (T={sysm.T}), tol 1e-12",
+           "batched_cand_per_s": B / (ms / 1e3), "ms_per_batch": ms,
+           "single_cand_per_s": n1 / (ms1 / 1e3), "ms_per_single": ms1 / n1,
+           "batched_speedup": (B / ms) / (n1 / ms1),
+           "max_abs_dE_batched_vs_single": float(max(single)),
+           "codes": np.bincount(err, minlength=3).tolist(), "iterations": np.bincount(it).tolist(),
+           "best_E": float(np.min(np.where(err == 0, E, np.inf))), "base_E": Eb}
+    if cpu:
+        out["cpu_baseline"] = cpu_candidates(sysm, params, cands, K0)
+    return out
+
+
+def cpu_candidates(sysm, params, cands, K0, Kp=600, ntrial=8):
+    """The oracle's sequential trial loop (all host threads) on a sample: a
+    base of K' functions, ntrial candidates, scaled to K by (K/K')^2 (one
+    trial is the row K of H, S, the bordered LDLHF row and O(K^2) inverse
+    iterations)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    o = orc.Oracle(sysm, Kp + 1)
+    o.set_params(params[:Kp])
+    o.last[:Kp] = 1.0
+    E0, _, _ = o.energy_ia(1, Kp, -1.2, -1e-12, max_iter=200)
+    lam = E0 * INVIT_PARAMETER
+    o.last[:Kp] = 1.0
+    o.energy_ia(1, Kp, lam, 1e-12)
+    start = np.zeros(Kp + 1, dtype=np.complex128)
+    start[:Kp] = o.last[:Kp]
+    t0 = time.perf_counter()
+    o.trial_loop(Kp, cands[:ntrial], lam, 1e-12, start)
+    t = (time.perf_counter() - t0) / ntrial * (K0 / Kp) ** 2
+    return {"value": 1.0 / t, "unit": "candidates/s", "cores": threads, "kind": "port",
+            "sample": f"oracle trial loop, {ntrial} candidates on a base of K'={Kp}, scaled by (K/K')^2"}
 
 
 def run_reference(args, dist):

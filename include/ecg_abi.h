@@ -180,6 +180,10 @@ int ecg_adjoint_gradient_noalloc(int n, const double* mass_matrix_host, const do
 /* Measured FP64 FMA throughput of the device (TFLOP/s, 2 flops per FMA):
  * a register-resident FMA loop over all SMs, timed with CUDA events. */
 int ecg_probe_fp64_peak(int device, double* tflops);
+/* Measured FP64 tensor-core throughput of the device (TFLOP/s, 2 flops per
+ * multiply-add): register-resident mma.sync.m8n8k4.f64 chains over all SMs,
+ * timed with CUDA events. */
+int ecg_probe_fp64_tensor_peak(int device, double* tflops);
 
 #ifdef __cplusplus
 }
