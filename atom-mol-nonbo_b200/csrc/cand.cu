@@ -85,7 +85,7 @@ template <int AMODE>
 __global__ void __launch_bounds__(256) k_zgemm(const cd* __restrict__ A, int lda, int M, int Kd,
                                                const cd* __restrict__ B, int ldb, cd* __restrict__ C, int ldc,
                                                const cd* __restrict__ E1, const cd* __restrict__ e2,
-                                               const int* __restrict__ cmap)
+                                               const int* __restrict__ cmap, cd* __restrict__ P, size_t pstride)
 {
     extern __shared__ double2 gsm[];
     const int i0 = blockIdx.x * GM, j0 = blockIdx.y * GN;
@@ -93,8 +93,13 @@ __global__ void __launch_bounds__(256) k_zgemm(const cd* __restrict__ A, int lda
     const int wm = (wp >> 2) * 32, wn = (wp & 3) * 16;
     ZAcc<4, 2> acc;
     acc.zero();
-    const int nk = (Kd + GK - 1) / GK;
-    auto stage = [&](int s, int kc) {
+    // split K: slice blockIdx.z of gridDim.z takes chunks [kc0, kc1)
+    const int nkt = (Kd + GK - 1) / GK;
+    const int per = (nkt + gridDim.z - 1) / gridDim.z;
+    const int kc0 = blockIdx.z * per, kc1 = min(nkt, kc0 + per);
+    const int nk = kc1 > kc0 ? kc1 - kc0 : 0;
+    auto stage = [&](int s, int kcl) {
+        const int kc = kc0 + kcl;
         double2* As = gsm + s * G_STAGE;
         double2* Bs = As + GK * G_LDA;
         const int k0 = kc * GK;
@@ -125,17 +130,18 @@ __global__ void __launch_bounds__(256) k_zgemm(const cd* __restrict__ A, int lda
         }
         cp_async_commit();
     };
-    stage(0, 0);
-    for (int kc = 0; kc < nk; kc++) {
-        if (kc + 1 < nk) {
-            stage((kc + 1) & 1, kc + 1);
+    if (nk > 0) stage(0, 0);
+    for (int kcl = 0; kcl < nk; kcl++) {
+        if (kcl + 1 < nk) {
+            stage((kcl + 1) & 1, kcl + 1);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
         }
         __syncthreads();
-        double2* As = gsm + (kc & 1) * G_STAGE;
+        double2* As = gsm + (kcl & 1) * G_STAGE;
         const double2* Bs = As + GK * G_LDA;
+        const int kc = kc0 + kcl;
         if (AMODE == 1 && i0 < (kc + 1) * GK) {
             // elements read from the upper triangle enter conjugated
             const int k0 = kc * GK;
@@ -161,6 +167,11 @@ __global__ void __launch_bounds__(256) k_zgemm(const cd* __restrict__ A, int lda
                 const int i = i0 + wm + mt * 8 + g;
                 const int j = j0 + wn + nt * 8 + 2 * t + e;
                 if (i >= M) continue;
+                if (gridDim.z > 1) {  // partial sum of this K slice, by slot
+                    *reinterpret_cast<double2*>(P + blockIdx.z * pstride + (size_t)i + (size_t)j * ldc) =
+                        make_double2(acc.r[mt][nt][e], acc.i[mt][nt][e]);
+                    continue;
+                }
                 const int jp = cmap ? cmap[j] : j;
                 cd v = mk(acc.r[mt][nt][e], acc.i[mt][nt][e]);
                 const size_t o = (size_t)i + (size_t)jp * ldc;
@@ -171,25 +182,96 @@ __global__ void __launch_bounds__(256) k_zgemm(const cd* __restrict__ A, int lda
 
 // ---------------------------------------------------------------------------
 // Multi-right-hand-side triangular solves with the base factor, one
-// cooperative launch each.  Work item (panel p, column block cb) of
-// CAND_NC columns; items are ordered so that every item depends only on
-// items with smaller indices, and each CTA takes items blockIdx.x,
-// blockIdx.x + gridDim.x, ... in order, so with all CTAs co-resident
-// every wait ends.  FWD (L y = w, then z = invD o y):
-//   Y_p = Linv_p (W_p - sum_{q<p} L_pq Y_q),  L_pq(m, k) = conj(U(q0+k, p0+m))
-// BWD (L^H x = z - U(:,K) x_K):
-//   X_p = Linv_p^H (Z_p - U(p,K) x_K - sum_{q>p} U_pq X_q)
-// with Linv_p the inverse unit-lower diagonal blocks of the factor.  Each
-// wait is bounded (CAND_SPIN_LIMIT polls, or at once after any CTA gave
-// up); a CTA that gives up records ST_SOLVE_TIMEOUT and publishes nothing.
+// cooperative launch each.  With Linv_p the inverse unit-lower diagonal
+// blocks of the factor and the off-diagonal blocks premultiplied once per
+// call (k_cand_gmat):
+//   FWD (L y = w, then z = invD o y):
+//     Y_p = Linv_p W_p - sum_{q<p} G_pq Y_q,           G_pq = Linv_p L_pq
+//   BWD (L^H x = z - U(:,K) x_K):
+//     X_p = Linv_p^H (Z_p - U(p,K) x_K) - sum_{q>p} G_pq X_q,  G_pq = Linv_p^H U_pq
+// (L_pq(m, k) = conj(U(q0+k, p0+m)), U_pq(m, k) = U(p0+m, q0+k)).  The
+// diagonal-block product needs no other panel, so it runs before the first
+// wait; each dependency's G tile (static) is loaded while the CTA waits for
+// that panel's flag, so a step of the panel chain is one flag hand-off, one
+// 64 x 16 tile load and one 64 x 64 x 16 product.
+// Work item (panel p, column block cb of CAND_NC columns); items are ordered
+// so that every item depends only on items with smaller indices, and each
+// CTA takes items blockIdx.x, blockIdx.x + gridDim.x, ... in order, so with
+// all CTAs co-resident every wait ends.  Each wait is bounded
+// (CAND_SPIN_LIMIT polls, or at once after any CTA gave up); a CTA that gives
+// up records ST_SOLVE_TIMEOUT and publishes nothing.
 // ---------------------------------------------------------------------------
 constexpr int CAND_SPIN_LIMIT = 1 << 22;
 constexpr int TS_LDA = 64 + 2;
 constexpr int TS_LDB = 64 + 4;
 constexpr size_t TS_SMEM = (size_t)(64 * TS_LDA + CAND_NC * TS_LDB) * sizeof(double2);
 
+// G tiles: one CTA per ordered panel pair (p, q), p != q; FWD blocks (p > q)
+// and BWD blocks (p < q) share the array, G(p0+m, q0+n) at Gm[(p0+m) + (q0+n) ld].
+__global__ void __launch_bounds__(256) k_cand_gmat(const cd* __restrict__ H, int ld, const int* __restrict__ bstart,
+                                                   int nb, const cd* __restrict__ linv, cd* __restrict__ Gm)
+{
+    extern __shared__ double2 gsm[];
+    const int p = blockIdx.x, q = blockIdx.y;
+    if (p == q || p >= nb || q >= nb) return;
+    const bool fwd = p > q;
+    const int p0 = bstart[p], bp = bstart[p + 1] - p0;
+    const int q0 = bstart[q], bq = bstart[q + 1] - q0;
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    const int wm = (wp >> 2) * 32, wn = (wp & 3) * 16;
+    ZAcc<4, 2> acc;
+    acc.zero();
+    double2* As = gsm;               // [k][m]: Linv_p (FWD) / Linv_p^H before its conjugation (BWD)
+    double2* Bs = gsm + GK * G_LDA;  // [n][k]: L_pq (FWD) / U_pq (BWD)
+    for (int k0 = 0; k0 < LDL_NB; k0 += GK) {
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int e = tid + 256 * u;
+            // A(m, k): FWD linv[(p0+m) 64 + k] (k contiguous); BWD conj(linv[(p0+k) 64 + m]) (m contiguous)
+            const int m = fwd ? (e >> 5) : (e & 63), k = fwd ? (e & 31) : (e >> 6);
+            const bool in = (m < bp) && (k0 + k < bp);
+            const cd* src = fwd ? linv + (size_t)(p0 + m) * LDL_NB + k0 + k : linv + (size_t)(p0 + k0 + k) * LDL_NB + m;
+            double2 v = make_double2(0.0, 0.0);
+            if (in) v = __ldg(reinterpret_cast<const double2*>(src));
+            As[k * G_LDA + m] = v;
+            // B(k, n): FWD conj(H[(q0+n) + (p0+k) ld]) (n contiguous); BWD H[(p0+k) + (q0+n) ld] (k contiguous)
+            const int n2 = fwd ? (e & 63) : (e >> 5), k2 = fwd ? (e >> 6) : (e & 31);
+            const bool in2 = (n2 < bq) && (k0 + k2 < bp);
+            double2 w = make_double2(0.0, 0.0);
+            if (in2) {
+                const cd* s2 = fwd ? H + (size_t)(q0 + n2) + (size_t)(p0 + k0 + k2) * ld
+                                   : H + (size_t)(p0 + k0 + k2) + (size_t)(q0 + n2) * ld;
+                w = __ldg(reinterpret_cast<const double2*>(s2));
+                if (fwd) w.y = -w.y;
+            }
+            Bs[n2 * G_LDB + k2] = w;
+        }
+        __syncthreads();
+        if (fwd) {
+#pragma unroll
+            for (int kk = 0; kk < GK; kk += 4) zmma_k4<4, 2, G_LDA, G_LDB, false>(acc, As, Bs, wm, wn, kk, lane);
+        } else {
+#pragma unroll
+            for (int kk = 0; kk < GK; kk += 4) zmma_k4<4, 2, G_LDA, G_LDB, true>(acc, As, Bs, wm, wn, kk, lane);
+        }
+        __syncthreads();
+    }
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < 4; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int m = wm + mt * 8 + g, n = wn + nt * 8 + 2 * t + e;
+                if (m < bp && n < bq)
+                    *reinterpret_cast<double2*>(Gm + (size_t)(p0 + m) + (size_t)(q0 + n) * ld) =
+                        make_double2(acc.r[mt][nt][e], acc.i[mt][nt][e]);
+            }
+}
+
 template <bool FWD>
-__global__ void __launch_bounds__(256) k_cand_solve(const cd* __restrict__ H, int ld, const int* __restrict__ bstart,
+__global__ void __launch_bounds__(256) k_cand_solve(const cd* __restrict__ Gm, int ld, const int* __restrict__ bstart,
                                                     int nb, const cd* __restrict__ linv, const cd* __restrict__ invD,
                                                     const cd* __restrict__ Win, cd* __restrict__ Yout,
                                                     cd* __restrict__ Zout, const cd* __restrict__ lcol,
@@ -206,14 +288,59 @@ __global__ void __launch_bounds__(256) k_cand_solve(const cd* __restrict__ H, in
     const int g = lane >> 2, t = lane & 3;
     const int nitems = nb * ncb;
     bool ok = true;
+    // G tile of dependency q into As (m contiguous in memory)
+    auto load_g = [&](int p0, int bp, int q) {
+        const int q0 = bstart[q], bq = bstart[q + 1] - q0;
+#pragma unroll 4
+        for (int u = 0; u < 16; u++) {
+            const int e = tid + 256 * u;
+            const int m = e & 63, k = e >> 6;
+            const bool in = (m < bp) && (k < bq);
+            cp_async16(As + k * TS_LDA + m, in ? Gm + (size_t)(p0 + m) + (size_t)(q0 + k) * ld : Gm, in ? 16 : 0);
+        }
+        cp_async_commit();
+    };
     for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
         const int pi = item / ncb, cb = item % ncb;
         const int p = FWD ? pi : nb - 1 - pi;
         const int p0 = bstart[p], bp = bstart[p + 1] - p0;
         const int col0 = cb * CAND_NC;
+        // (1) diagonal block: Linv_p rhs (FWD) / Linv_p^H (rhs - U(p,K) x_K) (BWD)
+#pragma unroll 4
+        for (int u = 0; u < 16; u++) {
+            const int e = tid + 256 * u;
+            const int m = FWD ? (e >> 6) : (e & 63);
+            const int k = FWD ? (e & 63) : (e >> 6);
+            const bool in = (m < bp) && (k < bp);
+            const cd* src = FWD ? linv + (size_t)(p0 + m) * LDL_NB + k : linv + (size_t)(p0 + k) * LDL_NB + m;
+            cp_async16(As + k * TS_LDA + m, in ? src : linv, in ? 16 : 0);
+        }
+        cp_async_commit();
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int e = tid + 256 * u;
+            const int m = e & 63, n = e >> 6;
+            cd v = mk(0.0, 0.0);
+            if (m < bp) {
+                const int jp = cmap ? cmap[col0 + n] : col0 + n;
+                const size_t o = (size_t)(p0 + m) + (size_t)jp * ldv;
+                v = ldcd(Win + o);
+                if (!FWD) v = cfms(ldcd(lcol + o), ldcd(xK + jp), v);
+            }
+            Bs[n * TS_LDB + m] = make_double2(v.x, v.y);
+        }
+        cp_async_wait<0>();
+        __syncthreads();
         ZAcc<2, 1> acc;
         acc.zero();
+#pragma unroll
+        for (int kk = 0; kk < 64; kk += 4) zmma_k4<2, 1, TS_LDA, TS_LDB, !FWD>(acc, As, Bs, wm, wn, kk, lane);
+        __syncthreads();
+        // (2) the panels this one depends on
+        ZAcc<2, 1> dep;
+        dep.zero();
         const int ndep = FWD ? p : nb - 1 - p;
+        if (ndep > 0) load_g(p0, bp, FWD ? 0 : nb - 1);
         for (int d = 0; d < ndep; d++) {
             const int q = FWD ? d : nb - 1 - d;
             if (tid == 0) {
@@ -238,16 +365,6 @@ __global__ void __launch_bounds__(256) k_cand_solve(const cd* __restrict__ H, in
                 break;
             }
             const int q0 = bstart[q], bq = bstart[q + 1] - q0;
-#pragma unroll 4
-            for (int u = 0; u < 16; u++) {
-                const int e = tid + 256 * u;
-                const int m = FWD ? (e >> 6) : (e & 63);
-                const int k = FWD ? (e & 63) : (e >> 6);
-                const bool in = (m < bp) && (k < bq);
-                const cd* src = FWD ? H + (size_t)(q0 + k) + (size_t)(p0 + m) * ld
-                                    : H + (size_t)(p0 + m) + (size_t)(q0 + k) * ld;
-                cp_async16(As + k * TS_LDA + m, in ? src : H, in ? 16 : 0);
-            }
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 const int e = tid + 256 * u;
@@ -260,43 +377,15 @@ __global__ void __launch_bounds__(256) k_cand_solve(const cd* __restrict__ H, in
             cp_async_wait<0>();
             __syncthreads();
 #pragma unroll
-            for (int kk = 0; kk < 64; kk += 4) zmma_k4<2, 1, TS_LDA, TS_LDB, FWD>(acc, As, Bs, wm, wn, kk, lane);
+            for (int kk = 0; kk < 64; kk += 4) zmma_k4<2, 1, TS_LDA, TS_LDB, false>(dep, As, Bs, wm, wn, kk, lane);
             __syncthreads();
+            if (d + 1 < ndep) load_g(p0, bp, FWD ? d + 1 : nb - 2 - d);  // overlaps the next wait
         }
-        if (!ok) break;
-        // right-hand side minus the accumulated panels -> B operand
-#pragma unroll
-        for (int mt = 0; mt < 2; mt++)
-#pragma unroll
-            for (int e = 0; e < 2; e++) {
-                const int m = wm + mt * 8 + g, n = wn + 2 * t + e;
-                cd v = mk(0.0, 0.0);
-                if (m < bp) {
-                    const int jp = cmap ? cmap[col0 + n] : col0 + n;
-                    const size_t o = (size_t)(p0 + m) + (size_t)jp * ldv;
-                    v = ldcd(Win + o);
-                    if (!FWD) v = cfms(ldcd(lcol + o), ldcd(xK + jp), v);
-                    v = v - mk(acc.r[mt][0][e], acc.i[mt][0][e]);
-                }
-                Bs[n * TS_LDB + m] = make_double2(v.x, v.y);
-            }
-        // inverse diagonal block: FWD Linv(m, k); BWD conj(Linv(k, m))
-#pragma unroll 4
-        for (int u = 0; u < 16; u++) {
-            const int e = tid + 256 * u;
-            const int m = FWD ? (e >> 6) : (e & 63);
-            const int k = FWD ? (e & 63) : (e >> 6);
-            const bool in = (m < bp) && (k < bp);
-            const cd* src = FWD ? linv + (size_t)(p0 + m) * LDL_NB + k : linv + (size_t)(p0 + k) * LDL_NB + m;
-            cp_async16(As + k * TS_LDA + m, in ? src : linv, in ? 16 : 0);
+        if (!ok) {
+            cp_async_wait<0>();
+            break;
         }
-        cp_async_commit();
-        cp_async_wait<0>();
-        __syncthreads();
-        ZAcc<2, 1> out;
-        out.zero();
-#pragma unroll
-        for (int kk = 0; kk < 64; kk += 4) zmma_k4<2, 1, TS_LDA, TS_LDB, !FWD>(out, As, Bs, wm, wn, kk, lane);
+        // (3) publish this panel
 #pragma unroll
         for (int mt = 0; mt < 2; mt++)
 #pragma unroll
@@ -305,7 +394,7 @@ __global__ void __launch_bounds__(256) k_cand_solve(const cd* __restrict__ H, in
                 if (m < bp) {
                     const int jp = cmap ? cmap[col0 + n] : col0 + n;
                     const size_t o = (size_t)(p0 + m) + (size_t)jp * ldv;
-                    const cd y = mk(out.r[mt][0][e], out.i[mt][0][e]);
+                    const cd y = mk(acc.r[mt][0][e] - dep.r[mt][0][e], acc.i[mt][0][e] - dep.i[mt][0][e]);
                     *reinterpret_cast<double2*>(Yout + o) = make_double2(y.x, y.y);
                     if (FWD) {
                         const cd z = cmul(y, ldcd(invD + p0 + m));
@@ -317,6 +406,23 @@ __global__ void __launch_bounds__(256) k_cand_solve(const cd* __restrict__ H, in
         __syncthreads();
         if (tid == 0) st_release_u32(flags + p * ncb + cb, 1u);
     }
+}
+
+// Split-K partial sums of k_zgemm are added in a fixed order:
+// C(:, slot j) = sum_z P[z](:, j) (+ E1 o e2), through the column map.
+__global__ void __launch_bounds__(256) k_zsum(const cd* __restrict__ P, int nz, size_t pstride, int M, int ncols,
+                                              int ldc, cd* __restrict__ C, const cd* __restrict__ E1,
+                                              const cd* __restrict__ e2, const int* __restrict__ cmap)
+{
+    const long long idx = (long long)blockIdx.x * 256 + threadIdx.x;
+    if (idx >= (long long)M * ncols) return;
+    const int i = (int)(idx % M), j = (int)(idx / M);
+    cd v = mk(0.0, 0.0);
+    for (int z = 0; z < nz; z++) v = v + ldcd(P + z * pstride + (size_t)i + (size_t)j * ldc);
+    const int jp = cmap ? cmap[j] : j;
+    const size_t o = (size_t)i + (size_t)jp * ldc;
+    if (E1) v = cfma(ldcd(E1 + o), ldcd(e2 + jp), v);
+    *reinterpret_cast<double2*>(C + o) = make_double2(v.x, v.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -634,6 +740,8 @@ int ensure_work(Ctx& c, int count)
     r |= dalloc_n(&cw.nd, (size_t)5 * ccap);
     r |= dalloc_n(&cw.st, (size_t)3 * ccap + 1);
     r |= dalloc_n(&cw.cmap, (size_t)ccap);
+    r |= dalloc_n(&cw.Gm, (size_t)c.ld * c.ld);
+    r |= dalloc_n(&cw.Pk, (size_t)CAND_KSPLIT * ldv * 2 * CAND_PAD);
     r |= dalloc_n(&cw.flags, (size_t)cw.nflags);
     r |= dalloc_n(&cw.bstart, (size_t)maxpanels + 1);
     r |= dalloc_n(&cw.abort_word, 1);
@@ -670,6 +778,8 @@ int solve_grid(Ctx& c)
     cudaFuncSetAttribute(k_cand_solve<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS_SMEM);
     cudaFuncSetAttribute(k_zgemm<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G_SMEM);
     cudaFuncSetAttribute(k_zgemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G_SMEM);
+    cudaFuncSetAttribute(k_cand_gmat, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(G_STAGE * sizeof(double2)));
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_cand_solve<true>, 256, TS_SMEM);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cand_solve<false>, 256, TS_SMEM);
     cudaGetLastError();
@@ -701,11 +811,11 @@ int launch_solve(Ctx& c, bool fwd, int nb, int ncols, const cd* Win, cd* Yout, c
     const cd* xk = cw.brd + BR_X * cw.ccap;
     cudaError_t e;
     if (fwd)
-        e = cudaLaunchKernelEx(&cfg, k_cand_solve<true>, (const cd*)c.H, c.ld, (const int*)cw.bstart, nb,
+        e = cudaLaunchKernelEx(&cfg, k_cand_solve<true>, (const cd*)cw.Gm, c.ld, (const int*)cw.bstart, nb,
                                (const cd*)c.linv, (const cd*)c.invD, Win, Yout, Zout, (const cd*)cw.Lcol, xk, cw.ldv,
                                ncb, cmap, cw.flags, c.status, cw.abort_word);
     else
-        e = cudaLaunchKernelEx(&cfg, k_cand_solve<false>, (const cd*)c.H, c.ld, (const int*)cw.bstart, nb,
+        e = cudaLaunchKernelEx(&cfg, k_cand_solve<false>, (const cd*)cw.Gm, c.ld, (const int*)cw.bstart, nb,
                                (const cd*)c.linv, (const cd*)c.invD, Win, Yout, Zout, (const cd*)cw.Lcol, xk, cw.ldv,
                                ncb, cmap, cw.flags, c.status, cw.abort_word);
     c.launches++;
@@ -717,12 +827,24 @@ int launch_gemm(Ctx& c, int amode, const cd* A, int M, int ncols, const cd* B, c
 {
     CandWork& cw = c.cand;
     if (M <= 0) return 0;
-    dim3 g((M + GM - 1) / GM, ncols / GN);
+    const int mt = (M + GM - 1) / GM, nt = ncols / GN;
+    // few output tiles (the late iterations run on one or two 64-column
+    // slots): split the inner dimension so that the GPU stays busy
+    int nz = 1;
+    if (ncols <= 2 * CAND_PAD) nz = std::max(1, std::min(CAND_KSPLIT, 148 / std::max(1, mt * nt)));
+    dim3 g(mt, nt, nz);
+    const size_t pstride = (size_t)cw.ldv * 2 * CAND_PAD;
     if (amode == 0)
-        k_zgemm<0><<<g, 256, G_SMEM, c.stream>>>(A, c.ld, M, M, B, cw.ldv, C, cw.ldv, E1, e2, cmap);
+        k_zgemm<0><<<g, 256, G_SMEM, c.stream>>>(A, c.ld, M, M, B, cw.ldv, C, cw.ldv, E1, e2, cmap, cw.Pk, pstride);
     else
-        k_zgemm<1><<<g, 256, G_SMEM, c.stream>>>(A, c.ld, M, M, B, cw.ldv, C, cw.ldv, E1, e2, cmap);
+        k_zgemm<1><<<g, 256, G_SMEM, c.stream>>>(A, c.ld, M, M, B, cw.ldv, C, cw.ldv, E1, e2, cmap, cw.Pk, pstride);
     c.launches++;
+    if (nz > 1) {
+        const long long cnt = (long long)M * ncols;
+        k_zsum<<<(unsigned)((cnt + 255) / 256), 256, 0, c.stream>>>(cw.Pk, nz, pstride, M, ncols, cw.ldv, C, E1, e2,
+                                                                    cmap);
+        c.launches++;
+    }
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
@@ -830,7 +952,8 @@ void cand_free(CandWork& cw)
 {
     drop_graphs(cw);
     void* ptrs[] = {cw.par, cw.bra, cw.ket, cw.det, cw.dS, cw.mu, cw.Mcol, cw.Scol, cw.Acol, cw.Lcol, cw.V, cw.W,
-                    cw.Y, cw.Z, cw.X, cw.X2, cw.brd, cw.nd, cw.st, cw.cmap, cw.flags, cw.bstart, cw.abort_word};
+                    cw.Y, cw.Z, cw.X, cw.X2, cw.brd, cw.nd, cw.st, cw.cmap, cw.Gm, cw.Pk, cw.flags, cw.bstart,
+                    cw.abort_word};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (cw.st_h) cudaFreeHost(cw.st_h);
@@ -902,6 +1025,12 @@ int eval_candidates(Ctx& c, int nbase, int count, const double* cand_host, doubl
     if ((r = CKc(cudaMemcpyAsync(cw.bstart, cw.bstart_h, sizeof(int) * (nb + 1), cudaMemcpyHostToDevice, c.stream))))
         return r;
     if (solve_grid(c) <= 0) return ECG_ECUDA;
+    // off-diagonal blocks premultiplied by the inverse diagonal blocks
+    if (nb > 1) {
+        k_cand_gmat<<<dim3(nb, nb), 256, G_STAGE * sizeof(double2), c.stream>>>(c.H, c.ld, cw.bstart, nb, c.linv,
+                                                                                 cw.Gm);
+        c.launches++;
+    }
     // bordered factor row: Acol = L0^-1 Mcol, Lcol = invD o Acol, then d_K
     if (launch_solve(c, true, nb, ncols, cw.Mcol, cw.Acol, cw.Lcol, nullptr)) return ECG_ECUDA;
     k_cand_border<<<count, 256, 0, c.stream>>>(cw.Acol, cw.Lcol, cw.mu, nbase, cw.ldv, cc, cw.brd, cw.st);

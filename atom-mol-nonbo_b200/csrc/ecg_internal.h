@@ -27,6 +27,8 @@ constexpr int CAND_ROW_SHAPES = 5;
 // the padding unit of the candidate column blocks.
 constexpr int CAND_NC = 16;
 constexpr int CAND_PAD = 64;
+// Largest split of the inner dimension of the candidates' GEMM.
+constexpr int CAND_KSPLIT = 4;
 
 // Workspace of the batched candidate evaluation (allocated on first use).
 // Column blocks are ldv x ccap, column j = candidate j, rows = base
@@ -38,6 +40,8 @@ struct CandWork {
     int ccap = 0;            // physical columns: bcap + CAND_PAD spare columns (stride of the per-column arrays)
     int ldv = 0;             // rows of the column blocks (ld rounded up to 64)
     int* cmap = nullptr;     // slot -> physical column of the active candidates (ccap)
+    cd* Gm = nullptr;        // ld x ld: off-diagonal factor blocks premultiplied by Linv (solves)
+    cd* Pk = nullptr;        // CAND_KSPLIT x ldv x 2 CAND_PAD: split-K partial sums of the GEMM
     double* par = nullptr;   // npt x bcap candidate parameters
     cd* bra = nullptr;       // bcap x NP
     cd* ket = nullptr;       // bcap x T x NP
