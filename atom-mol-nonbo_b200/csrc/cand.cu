@@ -1027,7 +1027,7 @@ int eval_candidates(Ctx& c, int nbase, int count, const double* cand_host, doubl
     if (solve_grid(c) <= 0) return ECG_ECUDA;
     // off-diagonal blocks premultiplied by the inverse diagonal blocks
     if (nb > 1) {
-        k_cand_gmat<<<dim3(nb, nb), 256, G_STAGE * sizeof(double2), c.stream>>>(c.H, c.ld, cw.bstart, nb, c.linv,
+        k_cand_gmat<<<dim3(nb, nb), 256, G_STAGE * sizeof(double2), c.stream>>>(c.F, c.ld, cw.bstart, nb, c.linv,
                                                                                  cw.Gm);
         c.launches++;
     }
@@ -1058,7 +1058,7 @@ int eval_candidates(Ctx& c, int nbase, int count, const double* cand_host, doubl
     }
     // Rayleigh quotients of the final iterates (all candidates)
     if (launch_gemm(c, 0, c.S, nbase, ncols, cw.V, cw.X, nullptr, nullptr, nullptr)) return ECG_ECUDA;
-    if (launch_gemm(c, 1, c.H, nbase, ncols, cw.V, cw.X2, nullptr, nullptr, nullptr)) return ECG_ECUDA;
+    if (launch_gemm(c, 1, c.F, nbase, ncols, cw.V, cw.X2, nullptr, nullptr, nullptr)) return ECG_ECUDA;
     k_cand_rayleigh<<<count, 256, 0, c.stream>>>(cw.X, cw.X2, cw.V, cw.Scol, cw.Mcol, cw.mu, nbase, cw.ldv, cc,
                                                  cw.brd, cw.nd, cw.st, approx_e);
     c.launches++;

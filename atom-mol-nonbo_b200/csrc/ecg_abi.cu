@@ -61,7 +61,9 @@ int dalloc(T** p, size_t count)
 
 void free_ctx(Ctx& c)
 {
-    void* ptrs[] = {c.params, c.H, c.S, c.diagS, c.diagH, c.invD, c.c, c.x, c.w, c.D, c.grad, c.Pd, c.coef,
+    if (c.F && c.F != c.H) cudaFree(c.F);
+    if (c.gcnt_h) cudaFreeHost(c.gcnt_h);
+    void* ptrs[] = {c.gcnt, c.params, c.H, c.S, c.diagS, c.diagH, c.invD, c.c, c.x, c.w, c.D, c.grad, c.Pd, c.coef,
                     c.bra, c.ket, c.detL, c.part, c.dw, c.linv, c.vbuf, c.status, c.red, c.counters, c.yv,
                     c.zv, c.spart, c.colval, c.dblk, c.flags};
     for (void* p : ptrs)
@@ -131,11 +133,11 @@ int compute_hsd(Ctx& c, int nmin, int nmax, int nfru, double approx_e)
     return 0;
 }
 
-// GHEPIIS, src/linalg.f90:1781-1926.
-int ghepiis(Ctx& c, int k, int n, double apprlambda, double tol, int max_iter, int specif_norm, double* lambda,
-            double* rel_acc, int* num_iter)
+// GHEPIIS, src/linalg.f90:1781-1926, on the factor matrix F (Glob_H in 'I'
+// contexts).
+int ghepiis_core(Ctx& c, int k, int n, double apprlambda, double tol, int max_iter, int specif_norm,
+                 double* lambda, double* rel_acc, int* num_iter)
 {
-    if (c.method != 'I') return ECG_EARG;
     if (k < 1 || n < k || n > c.ld || max_iter < 0) return ECG_EARG;
     *rel_acc = DBL_MAX;
     *num_iter = 0;
@@ -183,6 +185,156 @@ int ghepiis(Ctx& c, int k, int n, double apprlambda, double tol, int max_iter, i
         CKR(vec_scale(c, c.x, n, 1.0 / sqrt(c.red_h[RD_XX])));
     }
     return notconverged ? ECG_ENOCONV : ECG_OK;
+}
+
+int ghepiis(Ctx& c, int k, int n, double apprlambda, double tol, int max_iter, int specif_norm, double* lambda,
+            double* rel_acc, int* num_iter)
+{
+    if (c.method != 'I') return ECG_EARG;
+    return ghepiis_core(c, k, n, apprlambda, tol, max_iter, specif_norm, lambda, rel_acc, num_iter);
+}
+
+// ---------------------------------------------------------------------------
+// 'G' path: EnergyGA / EnergyGAM (src/workproc.f90:1697-1838).  The reference
+// mirrors H and S into full Hermitian matrices and calls ZHEGVX(ITYPE=1,
+// JOBZ, RANGE='I', IL=IU=which) (src/workproc.f90:1750): Cholesky of S (INFO
+// = n + i when its leading minor of order i is not positive definite), then
+// the which-th eigenvalue.  Here: the LDL^H pivots of S give the same test;
+// nu(sigma) = number of negative pivots of LDL^H(H - sigma S) = number of
+// eigenvalues below sigma (Sylvester's law of inertia) brackets the which-th
+// eigenvalue, bisection isolates it (nu(lo) = which - 1, nu(hi) = which),
+// and GHEPIIS at the bracket's centre converges to it, since every other
+// eigenvalue lies outside the bracket and so farther from its centre.
+// ---------------------------------------------------------------------------
+constexpr int G_MAX_FACT = 400;   // bound on the factorisations of one call
+constexpr int G_EXTRA_BISECT = 10;  // halvings after isolation: faster inverse iteration
+
+// nu(sigma) into *nu; *zero = 1 when a pivot was exactly zero
+int g_count(Ctx& c, int n, double sigma, int* nu, int* zero)
+{
+    CKR(g_shift(c, c.H, c.S, c.diagH, nullptr, n, sigma));
+    CK(cudaMemsetAsync(c.status, 0, ST_COUNT * sizeof(int), c.stream));
+    CKR(ldlh_factor(c, 0, n));
+    CKR(g_inertia(c, n));
+    CK(cudaMemcpyAsync(c.gcnt_h, c.gcnt, 2 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(c.status_h, c.status, ST_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    c.g_last_factorizations++;
+    *nu = c.gcnt_h[0];
+    *zero = c.status_h[ST_ZERO_PIVOT] != 0;
+    return 0;
+}
+
+int energy_ga(Ctx& c, int nmin, int nmax, int needed, int which, int want_vector, double* energy)
+{
+    if (c.method != 'G') return ECG_EARG;
+    if (nmin < 1 || nmax < nmin || nmax > c.ld || which < 1 || which > nmax) return ECG_EARG;
+    c.g_last_factorizations = 0;
+    if (needed) CKR(compute_hs(c, nmin, nmax, 0.0));
+    const int n = nmax;
+    if (n == 1) {  // EnergyGA's one-function branch: E = Glob_diagH(1)
+        double h;
+        CK(cudaMemcpyAsync(&h, c.diagH, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        const cd one{1.0, 0.0};
+        if (want_vector) CK(cudaMemcpyAsync(c.c, &one, sizeof(cd), cudaMemcpyHostToDevice, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+        *energy = h;
+        return ECG_OK;
+    }
+    CKR(g_mirror_s(c, n));
+    // S positive definite?  (ZPOTRF inside ZHEGVX: INFO = n + i)
+    CKR(g_shift(c, c.S, nullptr, nullptr, nullptr, n, 0.0));
+    CK(cudaMemsetAsync(c.status, 0, ST_COUNT * sizeof(int), c.stream));
+    CKR(ldlh_factor(c, 0, n));
+    CKR(g_inertia(c, n));
+    CK(cudaMemcpyAsync(c.gcnt_h, c.gcnt, 2 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    c.g_last_factorizations++;
+    if (c.gcnt_h[1] < n) return n + c.gcnt_h[1] + 1;
+    // initial bracket around the previous eigenvalue, or below min diag(H)
+    // (the lowest eigenvalue is at most every diagonal Rayleigh quotient)
+    double center, delta;
+    if (c.g_last_which == which) {
+        center = c.g_last_e;
+        delta = 1e-6 * std::max(1.0, fabs(center));
+    } else {
+        std::vector<double> dh(n);
+        CK(cudaMemcpyAsync(dh.data(), c.diagH, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+        center = *std::min_element(dh.begin(), dh.end());
+        delta = 1e-3 * std::max(1.0, fabs(center));
+    }
+    int nu = 0, zero = 0;
+    double lo = center - delta, hi = center + delta;
+    int nlo, nhi;
+    auto count = [&](double& s, int* v) -> int {
+        // an exactly zero pivot leaves the count undefined: move sigma by a few ulps
+        for (int tries = 0; tries < 8; tries++) {
+            const int r = g_count(c, n, s, v, &zero);
+            if (r) return r;
+            if (!zero) return 0;
+            s = s + (fabs(s) + 1e-300) * 1e-14 * (tries + 1);
+        }
+        return ECG_ENOCONV;
+    };
+    int r;
+    if ((r = count(lo, &nlo))) return r;
+    for (double d = delta; nlo >= which; ) {
+        d *= 4.0;
+        lo = center - d;
+        if ((r = count(lo, &nlo))) return r;
+        if (c.g_last_factorizations > G_MAX_FACT) return ECG_ENOCONV;
+    }
+    if ((r = count(hi, &nhi))) return r;
+    for (double d = delta; nhi < which; ) {
+        d *= 4.0;
+        hi = center + d;
+        if ((r = count(hi, &nhi))) return r;
+        if (c.g_last_factorizations > G_MAX_FACT) return ECG_ENOCONV;
+    }
+    // bisect until the bracket holds the which-th eigenvalue alone, then a
+    // few halvings more
+    int extra = 0;
+    for (;;) {
+        const bool isolated = (nlo == which - 1) && (nhi == which);
+        if (isolated && extra >= G_EXTRA_BISECT) break;
+        if (hi - lo <= 4.0 * DBL_EPSILON * std::max(fabs(lo), fabs(hi))) break;
+        if (c.g_last_factorizations > G_MAX_FACT) return ECG_ENOCONV;
+        double mid = 0.5 * (lo + hi);
+        if ((r = count(mid, &nu))) return r;
+        if (nu >= which) {
+            hi = mid;
+            nhi = nu;
+        } else {
+            lo = mid;
+            nlo = nu;
+        }
+        if (isolated) extra++;
+    }
+    // inverse iteration at the centre of the isolating bracket
+    double sigma = 0.5 * (lo + hi);
+    CKR(g_shift(c, c.H, c.S, c.diagH, nullptr, n, sigma));
+    if (c.g_last_which > 0) {
+        CK(cudaMemcpyAsync(c.c, c.x, (size_t)n * sizeof(cd), cudaMemcpyDeviceToDevice, c.stream));
+    } else {
+        std::vector<cd> ones(n, cd{1.0, 0.0});
+        CK(cudaMemcpyAsync(c.c, ones.data(), (size_t)n * sizeof(cd), cudaMemcpyHostToDevice, c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+    }
+    double lam = 0.0, ra = 0.0;
+    int it = 0;
+    const int e = ghepiis_core(c, 1, n, sigma, 1e-12, 20, want_vector ? 0 : -1, &lam, &ra, &it);
+    c.g_last_factorizations++;
+    if (e < 0) return e;
+    if (e == ECG_ESINGULAR) return ECG_ENOCONV;
+    // the converged eigenvalue is the bracket's; otherwise the bisection's own estimate
+    *energy = (lam >= lo && lam <= hi) ? lam : sigma;
+    c.last_numiter = it;
+    if (want_vector) CK(cudaMemcpyAsync(c.c, c.x, (size_t)n * sizeof(cd), cudaMemcpyDeviceToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    c.g_last_e = *energy;
+    c.g_last_which = which;
+    return ECG_OK;
 }
 
 int single_function_energy(Ctx& c, double approx_e, double* energy)
@@ -324,6 +476,11 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
     r |= dalloc(&c.params, (size_t)c.npt * L);
     r |= dalloc(&c.H, L * L);
     r |= dalloc(&c.S, L * L);
+    if (method == 'G')
+        r |= dalloc(&c.F, L * L);
+    else
+        c.F = c.H;
+    r |= dalloc(&c.gcnt, (size_t)4);
     r |= dalloc(&c.diagS, L);
     r |= dalloc(&c.diagH, L);
     r |= dalloc(&c.invD, L);
@@ -351,7 +508,8 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
     if (!r) {
         if (cudaMallocHost((void**)&c.status_h, ST_COUNT * sizeof(int)) != cudaSuccess ||
             cudaMallocHost((void**)&c.bounds_h, (L + 2) * sizeof(int)) != cudaSuccess ||
-            cudaMallocHost((void**)&c.red_h, RD_COUNT * sizeof(double)) != cudaSuccess) {
+            cudaMallocHost((void**)&c.red_h, RD_COUNT * sizeof(double)) != cudaSuccess ||
+            cudaMallocHost((void**)&c.gcnt_h, 4 * sizeof(int)) != cudaSuccess) {
             cudaGetLastError();
             r = ECG_ENOMEM;
         }
@@ -501,6 +659,36 @@ int ecg_eval_candidates(ecg_ctx* ctx, int nbase, int count, const double* cand_h
     if (cudaSetDevice(c.dev) != cudaSuccess) return ECG_ECUDA;
     return eval_candidates(c, nbase, count, cand_host, approx_energy, tol, max_iter, energies_host, errcodes_host,
                            num_iter_host, rel_acc_host);
+}
+
+int ecg_energy_ga(ecg_ctx* ctx, int nmin, int nmax, int mat_elem_needed, int which, int want_vector, double* energy,
+                  int* num_factorizations)
+{
+    if (!ctx || !energy) return ECG_EARG;
+    Ctx& c = ctx->c;
+    const int r = energy_ga(c, nmin, nmax, mat_elem_needed, which, want_vector, energy);
+    if (num_factorizations) *num_factorizations = c.g_last_factorizations;
+    return r;
+}
+
+int ecg_energy_gb_adjoint(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, int which, double* energy,
+                          double* grad_host)
+{
+    if (!ctx || !energy) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (c.method != 'G' || nfru < 0 || nfa <= nfru || nfa > c.ld) return ECG_EARG;
+    if (mat_elem_needed) CKR(compute_hs(c, nfru + 1, nfa, 0.0));
+    const int r = energy_ga(c, nfru + 1, nfa, 0, which, 1, energy);
+    if (r != ECG_OK) return r;
+    CKR(launch_adjoint(c, nfru, nfa, *energy));
+    const int nfo = nfa - nfru;
+    if (grad_host) {
+        CK(cudaMemcpyAsync(grad_host, c.grad, (size_t)nfo * c.npt * sizeof(double), cudaMemcpyDeviceToHost,
+                           c.stream));
+        c.bytes_d2h += (long long)nfo * c.npt * sizeof(double);
+    }
+    CK(cudaStreamSynchronize(c.stream));
+    return ECG_OK;
 }
 
 int ecg_get_matrices(ecg_ctx* ctx, int n, double* H_host, double* S_host, int ld_host, double* diagS_host,

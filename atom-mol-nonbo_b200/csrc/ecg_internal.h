@@ -93,6 +93,11 @@ struct Ctx {
     // Glob_* state, device resident
     double* params = nullptr;   // npt x ld, column-major (Glob_NonlinParam)
     cd* H = nullptr;            // ld x ld column-major (Glob_H)
+    // The matrix the LDL^H factorisation and the inverse iterations work on:
+    // Glob_H itself in 'I' contexts (H - lambda~ S in its lower triangle), a
+    // separate ld x ld array in 'G' contexts, where it holds H - sigma S for
+    // the shifts of the eigenvalue bisection and Glob_H keeps the 'G' layout.
+    cd* F = nullptr;
     cd* S = nullptr;            // ld x ld column-major (Glob_S)
     double* diagS = nullptr;    // Glob_diagS
     double* diagH = nullptr;    // Glob_diagH
@@ -153,6 +158,13 @@ struct Ctx {
     int last_numiter = 0;
 
     CandWork cand;           // batched candidate evaluation
+
+    // 'G' path (ZHEGVX semantics by inertia bisection)
+    int* gcnt = nullptr;     // device: [0] negative pivots, [1] first non-positive pivot (n = none)
+    int* gcnt_h = nullptr;   // pinned host mirror
+    double g_last_e = 0.0;   // last eigenvalue found, and its index
+    int g_last_which = 0;
+    int g_last_factorizations = 0;
 };
 
 enum StatusWord {
@@ -187,6 +199,11 @@ int launch_cand_rows(Ctx& c, CandWork& cw, int nbase, int count, double approx_e
 int eval_candidates(Ctx& c, int nbase, int count, const double* cand_host, double approx_e, double tol,
                     int max_iter, double* energies, int* errcodes, int* num_iter, double* rel_acc);
 void cand_free(CandWork& cw);
+
+// ---- 'G' path (gpath.cu kernels; driver energy_ga in ecg_abi.cu) ----
+int g_shift(Ctx& c, const cd* A, const cd* B, const double* dA, const double* dB, int n, double sigma);
+int g_mirror_s(Ctx& c, int n);
+int g_inertia(Ctx& c, int n);
 
 // ---- launchers (ldlh.cu) ----
 int ldlh_factor(Ctx& c, int m0, int n);

@@ -500,7 +500,7 @@ static int solve_multi_launch(Ctx& c, int n)
         int G = (j0 + 127) / 128;
         G = G < 1 ? 1 : (G > SOLVE_G_MAX ? SOLVE_G_MAX : G);
         const int chunk = (j0 + G - 1) / G;
-        k_fwd<<<G, 256, 0, c.stream>>>(c.H, c.ld, j0, j1, chunk > 0 ? chunk : 1, c.w, c.yv, c.zv, c.invD, c.linv,
+        k_fwd<<<G, 256, 0, c.stream>>>(c.F, c.ld, j0, j1, chunk > 0 ? chunk : 1, c.w, c.yv, c.zv, c.invD, c.linv,
                                       c.spart, c.counters);
         c.launches++;
     }
@@ -510,7 +510,7 @@ static int solve_multi_launch(Ctx& c, int n)
         int G = (rest + 127) / 128;
         G = G < 1 ? 1 : (G > SOLVE_G_MAX ? SOLVE_G_MAX : G);
         const int chunk = (rest + G - 1) / G;
-        k_bwd<<<G, 256, 0, c.stream>>>(c.H, c.ld, j0, j1, n, chunk > 0 ? chunk : 1, c.zv, c.x, c.linv, c.spart,
+        k_bwd<<<G, 256, 0, c.stream>>>(c.F, c.ld, j0, j1, n, chunk > 0 ? chunk : 1, c.zv, c.x, c.linv, c.spart,
                                       c.counters + 1);
         c.launches++;
     }
@@ -524,7 +524,7 @@ static int solve_cooperative(Ctx& c, int n)
     int* abort_word = c.counters + 2;
     if (cudaMemsetAsync(abort_word, 0, sizeof(int), c.stream) != cudaSuccess) return -2;
     const int* bs = c.dblk;
-    const cd* H = c.H;
+    const cd* H = c.F;
     const cd* w = c.w;
     const cd* invD = c.invD;
     const cd* linv = c.linv;
@@ -557,7 +557,7 @@ int invit_step(Ctx& c, int n, bool /*first*/)
 int invit_rayleigh(Ctx& c, int n)
 {
     dim3 g((n * 32 + 255) / 256, 2);
-    k_vmm_cols<<<g, 256, 0, c.stream>>>(c.S, c.H, c.ld, n, c.x, c.colval);
+    k_vmm_cols<<<g, 256, 0, c.stream>>>(c.S, c.F, c.ld, n, c.x, c.colval);
     k_vmm_reduce<<<1, 1024, 0, c.stream>>>(n, c.colval, c.x, c.red);
     c.launches += 2;
     return cudaGetLastError() == cudaSuccess ? 0 : -2;

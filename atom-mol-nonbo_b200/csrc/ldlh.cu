@@ -473,10 +473,10 @@ static void launch_update(Ctx& c, cudaStream_t st, const cd* vb, int p0, int p1,
         // one panel of rows (the lookahead rows): narrow 64 x 16 tiles so
         // that enough CTAs run
         dim3 g((n - c0 + 15) / 16, 1);
-        k_ldl_update<16, 8, 1><<<g, 256, UPD_SMEM, st>>>(c.H, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
+        k_ldl_update<16, 8, 1><<<g, 256, UPD_SMEM, st>>>(c.F, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
     } else {
         dim3 g((n - c0 + LDL_NB - 1) / LDL_NB, nrb);
-        k_ldl_update<64, 2, 4><<<g, 256, UPD_SMEM, st>>>(c.H, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
+        k_ldl_update<64, 2, 4><<<g, 256, UPD_SMEM, st>>>(c.F, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
     }
     c.launches++;
 }
@@ -490,14 +490,14 @@ static void enqueue_factor(Ctx& c, int m0, int n, const std::vector<int>& starts
     if (n > m0) {
         const int ct0 = m0 / 32, ct1 = (n + 31) / 32;
         dim3 g(ct1 - ct0, ct1);
-        k_ldl_mirror<<<g, 256, 0, c.stream>>>(c.H, c.ld, m0, n, c.dw, ct0);
+        k_ldl_mirror<<<g, 256, 0, c.stream>>>(c.F, c.ld, m0, n, c.dw, ct0);
         c.launches++;
     }
     // existing panels (bordered update): apply them to the new columns in order
     for (int i = 0; i < nexist; i++) {
         const int p0 = starts[i], p1 = std::min(blk_end(i), m0);
         if (p1 <= p0 || m0 >= n) continue;
-        k_ldl_trsm<<<(n - m0 + TRSM_COLS - 1) / TRSM_COLS, 256, sm1, c.stream>>>(c.H, c.ld, p0, p1, m0, n, c.invD,
+        k_ldl_trsm<<<(n - m0 + TRSM_COLS - 1) / TRSM_COLS, 256, sm1, c.stream>>>(c.F, c.ld, p0, p1, m0, n, c.invD,
                                                                                 c.vbuf);
         c.launches++;
         launch_update(c, c.stream, c.vbuf, p0, p1, p1, n, m0, n);
@@ -517,10 +517,10 @@ static void enqueue_factor(Ctx& c, int m0, int n, const std::vector<int>& starts
         const int p2 = (i + 1 < nblk) ? blk_end(i + 1) : n;
         const int p3 = (i + 2 < nblk) ? blk_end(i + 2) : n;
         cd* vb = c.vbuf + (size_t)((i - nexist) % 3) * LDL_NB * c.ld;
-        k_ldl_diag<<<1, 256, DG_SMEM, c.stream>>>(c.H, c.ld, p0, p1, c.dw, c.invD, c.status);
+        k_ldl_diag<<<1, 256, DG_SMEM, c.stream>>>(c.F, c.ld, p0, p1, c.dw, c.invD, c.status);
         c.launches++;
         if (p1 >= n) break;
-        k_ldl_trsm<<<(n - p1 + TRSM_COLS - 1) / TRSM_COLS, 256, sm1, c.stream>>>(c.H, c.ld, p0, p1, p1, n, c.invD, vb);
+        k_ldl_trsm<<<(n - p1 + TRSM_COLS - 1) / TRSM_COLS, 256, sm1, c.stream>>>(c.F, c.ld, p0, p1, p1, n, c.invD, vb);
         c.launches++;
         cudaEventRecord(c.lev[0], c.stream);
         // rows of the next panel wait for the previous trailing update's first part
@@ -538,7 +538,7 @@ static void enqueue_factor(Ctx& c, int m0, int n, const std::vector<int>& starts
         cudaStreamWaitEvent(c.stream, c.lev[0], 0);
     }
     if (nblk > nexist) {
-        k_ldl_linv<<<nblk - nexist, 256, 2 * sm1, c.stream>>>(c.H, c.ld, c.dblk, nexist, c.linv);
+        k_ldl_linv<<<nblk - nexist, 256, 2 * sm1, c.stream>>>(c.F, c.ld, c.dblk, nexist, c.linv);
         c.launches++;
     }
 }

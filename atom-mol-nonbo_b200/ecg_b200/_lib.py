@@ -29,6 +29,8 @@ PROTOTYPES = {
                                         _dp, _ip]),
     "ecg_eval_candidates": (C.c_int, [_vp, C.c_int, C.c_int, _dp, C.c_double, C.c_double, C.c_int, _dp, _ip, _ip,
                                       _dp]),
+    "ecg_energy_ga": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _ip]),
+    "ecg_energy_gb_adjoint": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]),
     "ecg_get_matrices": (C.c_int, [_vp, C.c_int, _dp, _dp, C.c_int, _dp, _dp, _dp]),
     "ecg_get_vectors": (C.c_int, [_vp, C.c_int, _dp, _dp]),
     "ecg_set_vectors": (C.c_int, [_vp, C.c_int, _dp, _dp]),

@@ -151,6 +151,24 @@ class Context:
         return self._energy_ib(self.lib.ecg_energy_ib_adjoint, "ecg_energy_ib_adjoint", nfru, nfa, approx_energy,
                                tol, max_iter, mat_elem_needed, want_grad)
 
+    def energy_ga(self, nmin, nmax, which=1, want_vector=False, mat_elem_needed=True):
+        """EnergyGA / EnergyGAM (src/workproc.f90:1697-1838) for a 'G'
+        context: the which-th eigenvalue with ZHEGVX(RANGE='I') semantics.
+        Returns (E, ErrorCode, number of LDL^H factorisations)."""
+        e, nf = C.c_double(), C.c_int()
+        err = _check(self.lib.ecg_energy_ga(self.h, int(nmin), int(nmax), int(bool(mat_elem_needed)), int(which),
+                                            int(bool(want_vector)), C.byref(e), C.byref(nf)), "ecg_energy_ga")
+        return e.value, err, nf.value
+
+    def energy_gb_adjoint(self, nfru, nfa, which=1, mat_elem_needed=True):
+        """EnergyGB (src/workproc.f90:1841-1950) through the fused adjoint
+        pass.  Returns (E, gradient, ErrorCode)."""
+        e = C.c_double()
+        g = np.zeros((nfa - nfru) * self.npt)
+        err = _check(self.lib.ecg_energy_gb_adjoint(self.h, int(nfru), int(nfa), int(bool(mat_elem_needed)),
+                                                    int(which), C.byref(e), dptr(g)), "ecg_energy_gb_adjoint")
+        return e.value, g, err
+
     def eval_candidates(self, nbase, candidates, approx_energy, tol, max_iter=20):
         """The BasisEnlI trial loop (src/workproc.f90:4054-4070) for a batch:
         for each row of `candidates` (count, npt), the energy of

@@ -9,6 +9,8 @@
 !   EnergyIA / EnergyIAM               -> GPU_EnergyIA(Nmin,Nmax,AreMatElemNeeded,SpecifNorm,ErrorCode)
 !   EnergyIB                           -> GPU_EnergyIB(Evalue,Gradient,AreMatElemNeeded,ErrorCode)
 !   BasisEnlI trial loop (Kstep = 1)   -> GPU_EvalTrials(nfru,NTrials,ParSets,Energies,ErrorCodes)
+!   EnergyGA / EnergyGAM               -> GPU_EnergyGA(Nmin,Nmax,AreMatElemNeeded,WantVector,ErrorCode)
+!   EnergyGB                           -> GPU_EnergyGB(Evalue,Gradient,AreMatElemNeeded,ErrorCode)
 !
 !The Glob_* matrices live on the GPU inside the context; GPU_GetMatrices
 !copies Glob_H/Glob_S/Glob_diagS/Glob_invD back where host code (pruning,
@@ -92,6 +94,22 @@ interface
     real(c_double), value :: approx_energy, tol
     real(c_double), intent(out) :: energies(*), rel_acc(*)
     integer(c_int), intent(out) :: errcodes(*), num_iter(*)
+  end function
+  integer(c_int) function ecg_energy_ga(ctx, nmin, nmax, needed, which, want_vector, energy, nfact) &
+      bind(C, name='ecg_energy_ga')
+    import :: c_int, c_double, c_ptr
+    type(c_ptr), value :: ctx
+    integer(c_int), value :: nmin, nmax, needed, which, want_vector
+    real(c_double), intent(out) :: energy
+    integer(c_int), intent(out) :: nfact
+  end function
+  integer(c_int) function ecg_energy_gb_adjoint(ctx, nfru, nfa, needed, which, energy, grad) &
+      bind(C, name='ecg_energy_gb_adjoint')
+    import :: c_int, c_double, c_ptr
+    type(c_ptr), value :: ctx
+    integer(c_int), value :: nfru, nfa, needed, which
+    real(c_double), intent(out) :: energy
+    real(c_double), intent(out) :: grad(*)
   end function
   integer(c_int) function ecg_get_matrices(ctx, n, H, S, ld, diagS, diagH, invD) bind(C, name='ecg_get_matrices')
     import :: c_int, c_double, c_ptr, c_double_complex
@@ -205,6 +223,36 @@ subroutine GPU_EvalTrials(nfru, NTrials, ParSets, Energies, ErrorCodes)
   Glob_InvItTempCounter1 = Glob_InvItTempCounter1 + NTrials
   Glob_InvItTempCounter2 = Glob_InvItTempCounter2 + sum(iters)
 end subroutine GPU_EvalTrials
+
+!EnergyGA (WantVector=.false.) / EnergyGAM (.true.), src/workproc.f90:1697,
+!for a context created with Glob_GSEPSolutionMethod='G': the
+!Glob_WhichEigenvalue-th eigenvalue with ZHEGVX(RANGE='I') semantics; with
+!WantVector, Glob_c (on the device) receives its eigenvector.
+function GPU_EnergyGA(Nmin, Nmax, AreMatElemNeeded, WantVector, ErrorCode)
+  real(dprec) :: GPU_EnergyGA
+  integer, intent(in) :: Nmin, Nmax
+  logical, intent(in) :: AreMatElemNeeded, WantVector
+  integer, intent(out) :: ErrorCode
+  integer(c_int) :: nf
+  real(c_double) :: e
+  if (AreMatElemNeeded) ErrorCode = ecg_set_params(ecg_ctx, Glob_NonlinParam, 1, Nmax)
+  ErrorCode = ecg_energy_ga(ecg_ctx, Nmin, Nmax, merge(1, 0, AreMatElemNeeded), Glob_WhichEigenvalue, &
+                            merge(1, 0, WantVector), e, nf)
+  GPU_EnergyGA = e
+  Glob_EnergyGACounter = Glob_EnergyGACounter + 1
+end function GPU_EnergyGA
+
+!EnergyGB, src/workproc.f90:1841, through the fused adjoint pass
+subroutine GPU_EnergyGB(Evalue, Gradient, AreMatElemNeeded, ErrorCode)
+  real(dprec), intent(out) :: Evalue
+  real(dprec), intent(out) :: Gradient(Glob_npt*Glob_nfo)
+  logical, intent(in) :: AreMatElemNeeded
+  integer, intent(out) :: ErrorCode
+  if (AreMatElemNeeded) ErrorCode = ecg_set_params(ecg_ctx, Glob_NonlinParam, 1, Glob_nfa)
+  ErrorCode = ecg_energy_gb_adjoint(ecg_ctx, Glob_nfru, Glob_nfa, merge(1, 0, AreMatElemNeeded), &
+                                    Glob_WhichEigenvalue, Evalue, Gradient)
+  Glob_EnergyGBCounter = Glob_EnergyGBCounter + 1
+end subroutine GPU_EnergyGB
 
 !Copy the device matrices and vectors back into the Glob_* host arrays for
 !code that still reads them on the host.

@@ -122,6 +122,29 @@ int ecg_eval_candidates(ecg_ctx* ctx, int nbase, int count, const double* cand_h
                         double tol, int max_iter, double* energies_host, int* errcodes_host, int* num_iter_host,
                         double* rel_acc_host);
 
+/* EnergyGA (want_vector 0) / EnergyGAM (want_vector 1), src/workproc.f90:
+ * 1697-1838, for contexts created with method 'G': optional
+ * ComputeMatElem(Nmin,Nmax), then the which-th smallest eigenvalue of
+ * H c = E S c with the semantics of the reference's
+ * ZHEGVX(1, JOBZ, 'I', 'U', Nmax, ..., IL=IU=which) (src/workproc.f90:1750);
+ * with want_vector, Glob_c = its eigenvector normalised c^H S c = 1.  As in
+ * the reference, Glob_S's upper triangle is filled from its lower one.
+ * Method: LDL^H of S for the positive-definiteness test; Sylvester-inertia
+ * bisection on LDL^H(H - sigma S) (negative pivots = eigenvalues below
+ * sigma) until the bracket holds the which-th eigenvalue alone; GHEPIIS at
+ * the bracket's centre.  num_factorizations (may be NULL) receives the
+ * number of LDL^H factorisations used.  Returns 0, or Nmax + i when the
+ * leading minor of order i of S is not positive definite (ZHEGVX's INFO),
+ * or a negative status. */
+int ecg_energy_ga(ecg_ctx* ctx, int nmin, int nmax, int mat_elem_needed, int which, int want_vector, double* energy,
+                  int* num_factorizations);
+
+/* EnergyGB, src/workproc.f90:1841-1950, through the fused adjoint pass:
+ * optional ComputeMatElem(nfru+1, nfa), EnergyGAM's eigenpair, then the
+ * gradient of ecg_energy_ib_adjoint (same ordering) at that eigenpair. */
+int ecg_energy_gb_adjoint(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, int which, double* energy,
+                          double* grad_host);
+
 /* Device -> host copies of the context arrays (any pointer may be NULL).
  * H_host, S_host: n x n with leading dimension ld_host. */
 int ecg_get_matrices(ecg_ctx* ctx, int n, double* H_host, double* S_host, int ld_host, double* diagS_host,
