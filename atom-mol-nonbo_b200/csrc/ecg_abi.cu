@@ -715,6 +715,34 @@ int ecg_get_matrices(ecg_ctx* ctx, int n, double* H_host, double* S_host, int ld
     return ECG_OK;
 }
 
+int ecg_set_matrices(ecg_ctx* ctx, int n, const double* H_host, const double* S_host, int ld_host,
+                     const double* diagS_host, const double* diagH_host)
+{
+    if (!ctx || n < 0 || n > ctx->c.ld) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if ((H_host || S_host) && ld_host < n) return ECG_EARG;
+    const size_t w = (size_t)n * sizeof(cd);
+    if (n > 0) {
+        if (H_host)
+            CK(cudaMemcpy2DAsync(c.H, (size_t)c.ld * sizeof(cd), H_host, (size_t)ld_host * sizeof(cd), w, n,
+                                 cudaMemcpyHostToDevice, c.stream));
+        if (S_host)
+            CK(cudaMemcpy2DAsync(c.S, (size_t)c.ld * sizeof(cd), S_host, (size_t)ld_host * sizeof(cd), w, n,
+                                 cudaMemcpyHostToDevice, c.stream));
+        if (diagS_host)
+            CK(cudaMemcpyAsync(c.diagS, diagS_host, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        if (diagH_host)
+            CK(cudaMemcpyAsync(c.diagH, diagH_host, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        c.bytes_h2d += (long long)(H_host ? n * w : 0) + (S_host ? n * w : 0) + (diagS_host ? n * 8 : 0) +
+                       (diagH_host ? n * 8 : 0);
+    }
+    CK(cudaStreamSynchronize(c.stream));
+    // the matrices changed: no row of an earlier factor may be reused
+    c.fact_n = 0;
+    c.blk_start.clear();
+    return ECG_OK;
+}
+
 int ecg_get_vectors(ecg_ctx* ctx, int n, double* c_host, double* last_eigvec_host)
 {
     if (!ctx || n < 0 || n > ctx->c.ld) return ECG_EARG;

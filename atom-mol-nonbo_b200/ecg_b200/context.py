@@ -46,6 +46,7 @@ class Context:
         _check(self.lib.ecg_ctx_create(system.n, dptr(mm), dptr(ch), system.T, iptr(ym), iptr(yc), self.ld,
                                        int(max_nfo), method.encode(), int(device), C.byref(h)), "ecg_ctx_create")
         self.h = h
+        self.method = method
 
     # -- lifetime -----------------------------------------------------------
     def close(self):
@@ -82,6 +83,38 @@ class Context:
         _check(self.lib.ecg_get_matrices(self.h, n, H.ctypes.data_as(_lib._dp), S.ctypes.data_as(_lib._dp), n,
                                          dptr(dS), dptr(dH), iD.ctypes.data_as(_lib._dp)), "ecg_get_matrices")
         return H, S, dS, dH, iD
+
+    def set_matrices(self, H=None, S=None, diagS=None, diagH=None):
+        """Glob_H, Glob_S (n x n, the context's layout), Glob_diagS, Glob_diagH
+        into the context (ecg_set_matrices)."""
+        arrs = [None if a is None else np.asfortranarray(a, dtype=np.complex128) for a in (H, S)]
+        n = next(a.shape[0] for a in arrs + [diagS, diagH] if a is not None)
+        dS = None if diagS is None else np.ascontiguousarray(diagS, dtype=np.float64)
+        dH = None if diagH is None else np.ascontiguousarray(diagH, dtype=np.float64)
+        _check(self.lib.ecg_set_matrices(self.h, n, None if arrs[0] is None else arrs[0].ctypes.data_as(_lib._dp),
+                                         None if arrs[1] is None else arrs[1].ctypes.data_as(_lib._dp), n,
+                                         dptr(dS), dptr(dH)), "ecg_set_matrices")
+
+    def store_swap(self, path, n, approx_energy=0.0):
+        """StoreMatricesInSwapFile (src/workproc.f90:2244-2311): H and S of
+        the first n functions to the reference's swap file."""
+        from .inout import pack_swap, write_swap
+        H, S, dS, dH, _ = self.matrices(n)
+        write_swap(path, pack_swap(H, S, dH, self.method, approx_energy), dS)
+
+    def read_swap(self, path, n, approx_energy=0.0):
+        """ReadSwapFileAndDistributeData (src/workproc.f90:2158-2240): H and S
+        of n functions from the reference's swap file into the context, the
+        'I' layout shifted by approx_energy.  Returns False (and leaves the
+        context alone) when the file holds another basis size."""
+        from .inout import read_swap, unpack_swap
+        got = read_swap(path, n)
+        if got is None:
+            return False
+        P, dS = got
+        H, S, dH = unpack_swap(P, self.method, approx_energy)
+        self.set_matrices(H, S, dS, dH if self.method == "G" else None)
+        return True
 
     def vectors(self, n):
         c = np.zeros(n, dtype=np.complex128)

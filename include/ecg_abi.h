@@ -149,6 +149,14 @@ int ecg_energy_gb_adjoint(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, 
  * H_host, S_host: n x n with leading dimension ld_host. */
 int ecg_get_matrices(ecg_ctx* ctx, int n, double* H_host, double* S_host, int ld_host, double* diagS_host,
                      double* diagH_host, double* invD_host);
+/* The reverse of ecg_get_matrices: Glob_H, Glob_S (n x n, leading dimension
+ * ld_host), Glob_diagS and Glob_diagH from host memory (any pointer may be
+ * NULL), in the context's layout ('I' or 'G').  This is how the matrices
+ * of the reference's swap file come back (ReadSwapFileAndDistributeData,
+ * src/workproc.f90:2158-2240) so that EnergyIA / EnergyGA can run with
+ * mat_elem_needed = 0.  The LDL^H factor of earlier rows is discarded. */
+int ecg_set_matrices(ecg_ctx* ctx, int n, const double* H_host, const double* S_host, int ld_host,
+                     const double* diagS_host, const double* diagH_host);
 int ecg_get_vectors(ecg_ctx* ctx, int n, double* c_host, double* last_eigvec_host);
 int ecg_set_vectors(ecg_ctx* ctx, int n, const double* c_host, const double* last_eigvec_host);
 int ecg_get_gradient(ecg_ctx* ctx, int nfo, double* grad_host);

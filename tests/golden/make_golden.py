@@ -6,7 +6,8 @@ The reference ships six optimised HD+ bases with the energy each one gives
 keyword files -- the layout written by SaveResults, src/workproc.f90:436-571,
 and read by ReadIOFile, src/workproc.f90:18-433 -- and stores the system, the
 stored CURRENT_ENERGY, WHICH_EIGENVALUE, INVITPARAMETER, EIGVAL_TOLERANCE and
-the K x npt nonlinear parameters in hdplus_fixtures.npz.
+the K x npt nonlinear parameters in hdplus_fixtures.npz, and copies one of
+the files (inout_2_500.txt) unchanged for the data-file reader/writer tests.
 
 Run it in a checkout that has the reference at REFERENCE_ROOT (default
 /root/reference).  The GPU tests only read the .npz it writes.
@@ -19,6 +20,7 @@ import numpy as np
 REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 NAMES = [f"inout_{w}_{k}" for w in (1, 2) for k in (500, 1000, 1500)]
+TEXT_FIXTURE = "inout_2_500"
 
 
 def _num(tok):
@@ -63,6 +65,13 @@ def main():
             out[f"{name}/{key}"] = np.asarray(val)
     dst = os.path.join(HERE, "hdplus_fixtures.npz")
     np.savez_compressed(dst, **out)
+    print("wrote", dst, os.path.getsize(dst), "bytes")
+    # one data file verbatim, for the reader/writer round trip (SaveResults'
+    # exact text layout)
+    src = os.path.join(REF, "example_input", TEXT_FIXTURE + ".txt")
+    dst = os.path.join(HERE, TEXT_FIXTURE + ".txt")
+    with open(src) as fi, open(dst, "w") as fo:
+        fo.write(fi.read())
     print("wrote", dst, os.path.getsize(dst), "bytes")
 
 
