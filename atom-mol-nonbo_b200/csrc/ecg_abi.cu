@@ -458,7 +458,12 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
         cf[t] = yhy_coeffs_host[t];
     }
     int r = 0;
-    if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) {
+    // the context's stream carries the LDL^H panel chain; its higher
+    // priority lets the chain's CTAs take SMs ahead of the bulk trailing
+    // updates queued on the side stream
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    if (cudaStreamCreateWithPriority(&c.stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess) {
         cudaGetLastError();
         delete h;
         return ECG_ECUDA;
@@ -466,7 +471,7 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
     for (int i = 0; i < 16; i++) cudaEventCreate(&c.ev[i]);
     for (int i = 0; i < 2; i++) cudaEventCreate(&c.tev[i]);
     for (int i = 0; i < 2; i++) cudaEventCreateWithFlags(&c.lev[i], cudaEventDisableTiming);
-    if (cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithPriority(&c.side, cudaStreamNonBlocking, prio_lo) != cudaSuccess) {
         cudaGetLastError();
         free_ctx(c);
         delete h;

@@ -63,9 +63,8 @@ __global__ void __launch_bounds__(256) k_ldl_mirror(cd* __restrict__ A, int ld, 
 // Diagonal block elimination, blocked by 8-row sub-panels.  The working
 // 64 x 64 upper triangle W(r, c), r <= c (diagonal from dw), sits in shared
 // memory.  Per sub-panel (rows s0..s0+7):
-//   (a) eight lanes of warp 0 eliminate the 8 x 8 diagonal sub-block in
-//       registers (lane j holds column j; pivots and row values by
-//       shuffle);
+//   (a) one thread eliminates the 8 x 8 diagonal sub-block in its
+//       registers;
 //   (b) one thread per column c beyond the sub-block forms the unscaled
 //       rows Wun(q, c) = W(q, c) - sum_{q' < q} conj(U(q', q)) Wun(q', c)
 //       by substitution and U(q, c) = invD_q Wun(q, c);
@@ -106,43 +105,42 @@ __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, in
     __syncthreads();
     for (int s0 = 0; s0 < b; s0 += DG_SUB) {
         const int nq = min(DG_SUB, b - s0);
-        // (a) 8 x 8 diagonal sub-block
-        if (tid < 32) {
-            const int j = tid & 7;  // lanes 8..31 shadow lanes 0..7 (same values, no stores)
-            cd col[DG_SUB];
+        // (a) 8 x 8 diagonal sub-block, in the registers of one thread: no
+        // shuffles, so a pivot step costs one reciprocal and three dependent
+        // FP64 operations
+        if (tid == 0) {
+            cd a[DG_SUB][DG_SUB];
 #pragma unroll
-            for (int i = 0; i < DG_SUB; i++) {
-                const double2 v = (i <= j && j < nq) ? Ws[(s0 + i) * DG_LD + s0 + j] : make_double2(0.0, 0.0);
-                col[i] = cd{v.x, v.y};
-            }
+            for (int i = 0; i < DG_SUB; i++)
+#pragma unroll
+                for (int j = i; j < DG_SUB; j++) {
+                    const double2 v = (j < nq) ? Ws[(s0 + i) * DG_LD + s0 + j] : make_double2(0.0, 0.0);
+                    a[i][j] = cd{v.x, v.y};
+                }
 #pragma unroll
             for (int q = 0; q < DG_SUB; q++) {
-                if (q < nq) {  // warp-uniform
-                    const double dr = __shfl_sync(0xffffffffu, col[q].x, q);  // Re W(q, q)
+                if (q < nq) {
+                    const double dr = a[q][q].x;  // pivot d = conj(W(q,q)), real
                     const double id = (dr != 0.0) ? __drcp_rn(dr) : 0.0;
-                    if (tid == 0) {
-                        sid[q] = id;
-                        invD[p0 + s0 + q] = cd{id, 0.0};
-                        if (dr == 0.0) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + s0 + q + 1);
-                    }
-                    const cd wq = col[q];
+                    sid[q] = id;
+                    invD[p0 + s0 + q] = cd{id, 0.0};
+                    if (dr == 0.0) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + s0 + q + 1);
+                    cd u[DG_SUB];
 #pragma unroll
-                    for (int i = 1; i < DG_SUB; i++) {
-                        if (i > q) {
-                            cd w;  // W(q, i), held by lane i
-                            w.x = __shfl_sync(0xffffffffu, col[q].x, i);
-                            w.y = __shfl_sync(0xffffffffu, col[q].y, i);
-                            if (j >= i) col[i] = cfms(cd{w.x * id, -w.y * id}, wq, col[i]);
-                        }
-                    }
-                    if (j > q) col[q] = cd{wq.x * id, wq.y * id};
+                    for (int j = q + 1; j < DG_SUB; j++) u[j] = cd{a[q][j].x * id, a[q][j].y * id};  // U(q, j)
+#pragma unroll
+                    for (int i = q + 1; i < DG_SUB; i++)
+#pragma unroll
+                        for (int j = i; j < DG_SUB; j++) a[i][j] = cfms(conj(u[i]), a[q][j], a[i][j]);
+#pragma unroll
+                    for (int j = q + 1; j < DG_SUB; j++) a[q][j] = u[j];
                 }
             }
-            if (tid < 8) {
 #pragma unroll
-                for (int i = 0; i < DG_SUB; i++)
-                    if (i < j && j < nq) Ws[(s0 + i) * DG_LD + s0 + j] = make_double2(col[i].x, col[i].y);
-            }
+            for (int i = 0; i < DG_SUB; i++)
+#pragma unroll
+                for (int j = i + 1; j < DG_SUB; j++)
+                    if (j < nq) Ws[(s0 + i) * DG_LD + s0 + j] = make_double2(a[i][j].x, a[i][j].y);
         }
         __syncthreads();
         // (b) sub-panel rows beyond the sub-block, one thread per column
