@@ -457,6 +457,8 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
             for (int j = 0; j < n; j++) P[((size_t)t * NMAX + i) * NMAX + j] = yhy_mats_host[(size_t)t * n * n + i + j * n];
         cf[t] = yhy_coeffs_host[t];
     }
+    c.yhy_h.assign(yhy_mats_host, yhy_mats_host + (size_t)nterms * n * n);
+    c.yhy_coef_h.assign(yhy_coeffs_host, yhy_coeffs_host + nterms);
     int r = 0;
     // the context's stream carries the LDL^H panel chain; its higher
     // priority lets the chain's CTAs take SMs ahead of the bulk trailing
@@ -694,6 +696,50 @@ int ecg_energy_gb_adjoint(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, 
     }
     CK(cudaStreamSynchronize(c.stream));
     return ECG_OK;
+}
+
+int ecg_expectation_values(ecg_ctx* ctx, int nbasis, const double* masses_host, int symm_adapt_method, int ny,
+                           const int* y_mats_host, const int* y_coeffs_host, double energy, const double* c_host,
+                           int ncf, const double* cf_grid_host, int ndens, const double* dens_grid_host,
+                           double* values_host, double* errors_host, double* cf_host, double* dens_host)
+{
+    if (!ctx || !masses_host) return ECG_EARG;
+    Ctx& c = ctx->c;
+    const int n = c.n;
+    if (nbasis < 1 || nbasis > c.ld || ncf < 0 || ndens < 0) return ECG_EARG;
+    if ((ncf > 0 && !cf_grid_host) || (ndens > 0 && !dens_grid_host)) return ECG_EARG;
+    // term lists of src/workproc.f90:8175-8347
+    std::vector<int> pb, pk;
+    std::vector<double> c1, c2;
+    int em;
+    if (symm_adapt_method == 1) {
+        std::vector<int> eye((size_t)n * n, 0);
+        for (int i = 0; i < n; i++) eye[i + i * n] = 1;
+        for (int t = 0; t < c.T; t++) {
+            pb.insert(pb.end(), eye.begin(), eye.end());
+            pk.insert(pk.end(), c.yhy_h.begin() + (size_t)t * n * n, c.yhy_h.begin() + (size_t)(t + 1) * n * n);
+            c1.push_back(c.yhy_coef_h[t]);
+            c2.push_back(1.0);
+        }
+        em = 2;
+    } else if (symm_adapt_method == 2) {
+        if (ny < 1 || ny > 64 || !y_mats_host || !y_coeffs_host) return ECG_EARG;
+        for (int k = 0; k < ny; k++)
+            for (int kk = 0; kk < ny; kk++) {
+                pb.insert(pb.end(), y_mats_host + (size_t)k * n * n, y_mats_host + (size_t)(k + 1) * n * n);
+                pk.insert(pk.end(), y_mats_host + (size_t)kk * n * n, y_mats_host + (size_t)(kk + 1) * n * n);
+                c1.push_back(y_coeffs_host[k]);
+                c2.push_back(y_coeffs_host[kk]);
+            }
+        em = 3;
+    } else {
+        return ECG_EARG;
+    }
+    if (cudaSetDevice(c.dev) != cudaSuccess) return ECG_ECUDA;
+    const int r = expectation_values(c, nbasis, masses_host, (int)c1.size(), pb.data(), pk.data(), c1.data(),
+                                     c2.data(), em, energy, reinterpret_cast<const cd*>(c_host), ncf, cf_grid_host,
+                                     ndens, dens_grid_host, values_host, errors_host, cf_host, dens_host);
+    return r == 0 ? ECG_OK : (r == -3 ? ECG_ENOMEM : (r == -1 ? ECG_EARG : ECG_ECUDA));
 }
 
 int ecg_get_matrices(ecg_ctx* ctx, int n, double* H_host, double* S_host, int ld_host, double* diagS_host,

@@ -111,6 +111,8 @@ struct Ctx {
     // derived per-function data for the pair kernels
     double* Pd = nullptr;       // T x NMAX x NMAX permutation matrices (double, row-major)
     double* coef = nullptr;     // T coefficients (double)
+    std::vector<int> yhy_h;     // host copy of Glob_YHYMatr (n x n x T column-major)
+    std::vector<int> yhy_coef_h;  // host copy of Glob_YHYCoeff
     cd* bra = nullptr;          // ld x NP: Ck = A - iB packed (vech order)
     cd* ket = nullptr;          // ld x T x NP: P'AP + iP'BP packed
     double* detL = nullptr;     // ld
@@ -199,6 +201,14 @@ int launch_cand_rows(Ctx& c, CandWork& cw, int nbase, int count, double approx_e
 int eval_candidates(Ctx& c, int nbase, int count, const double* cand_host, double approx_e, double tol,
                     int max_iter, double* energies, int* errcodes, int* num_iter, double* rel_acc);
 void cand_free(CandWork& cw);
+
+// ---- expectation values (expc.cu) ----
+// The accumulation loop of ExpectationValuesG over functions 1..nbasis for
+// a term list (Pbra_t, Pket_t column-major n x n, weights coef1_t coef2_t).
+int expectation_values(Ctx& c, int nbasis, const double* masses, int nterms, const int* pbra, const int* pket,
+                       const double* coef1, const double* coef2, int err_mult, double energy, const cd* c_host,
+                       int ncf, const double* cf_grid, int ndens, const double* dens_grid, double* values,
+                       double* errors, double* cf, double* dens);
 
 // ---- 'G' path (gpath.cu kernels; driver energy_ga in ecg_abi.cu) ----
 int g_shift(Ctx& c, const cd* A, const cd* B, const double* dA, const double* dB, int n, double sigma);

@@ -4,6 +4,6 @@ solve of HC = ESC and the nonlinear-parameter gradient, behind the C ABI of
 include/ecg_abi.h.  This package is the Python mirror of that ABI."""
 from .system import System, expand_yhy, parse_young, transposition_matrix
 from .context import Context, EcgError, probe_fp64_peak, probe_fp64_tensor_peak
-from . import synth, inout
+from . import synth, inout, expc
 
-__all__ = ["System", "Context", "EcgError", "probe_fp64_peak", "probe_fp64_tensor_peak", "expand_yhy", "parse_young", "transposition_matrix", "synth", "inout"]
+__all__ = ["System", "Context", "EcgError", "probe_fp64_peak", "probe_fp64_tensor_peak", "expand_yhy", "parse_young", "transposition_matrix", "synth", "inout", "expc"]

@@ -10,7 +10,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import _lib
+from . import _lib, expc
 from ._lib import dptr, iptr
 
 __all__ = ["Context", "EcgError", "probe_fp64_peak", "probe_fp64_tensor_peak"]
@@ -201,6 +201,56 @@ class Context:
         err = _check(self.lib.ecg_energy_gb_adjoint(self.h, int(nfru), int(nfa), int(bool(mat_elem_needed)),
                                                     int(which), C.byref(e), dptr(g)), "ecg_energy_gb_adjoint")
         return e.value, g, err
+
+    def expectation_values(self, nbasis, energy, c=None, method=1, cf_grid=None, dens_grid=None, raw=False):
+        """The expectation-value pass of ExpectationValuesG
+        (src/workproc.f90:8159-8366) over functions 1..nbasis with the
+        eigenvector c (None: Glob_c, as left by energy_ga(want_vector=True))
+        and Glob_CurrEnergy = energy.  method is SymmAdaptMethod (1: Y^+Y on
+        the ket, 2: Y on bra and ket).  Returns a dict of named values and
+        error bounds (see expc.unpack) plus "cf" (np x ncf) and "dens"
+        ((n+1) x ndens) when grids are given; with raw=True the MEkl-ordered
+        (values, errors, cf, dens) arrays instead."""
+        sysm = self.system
+        n = sysm.n
+        nv = 6 * self.np + 9
+        vals, errs = np.zeros(nv), np.zeros(nv)
+        cfg = np.ascontiguousarray(cf_grid if cf_grid is not None else np.zeros(0), dtype=np.float64)
+        dg = np.ascontiguousarray(dens_grid if dens_grid is not None else np.zeros(0), dtype=np.float64)
+        cf = np.zeros((self.np, max(cfg.size, 1)), order="F")
+        dens = np.zeros((n + 1, max(dg.size, 1)), order="F")
+        masses = np.ascontiguousarray(sysm.masses, dtype=np.float64)
+        ym = np.ascontiguousarray(sysm.y_mats_cm, dtype=np.int32)
+        yc = np.ascontiguousarray(sysm.y_coeffs, dtype=np.int32)
+        cc = None
+        if c is not None:
+            cc = np.ascontiguousarray(np.asarray(c)[:nbasis], dtype=np.complex128).view(np.float64)
+        _check(self.lib.ecg_expectation_values(self.h, int(nbasis), dptr(masses), int(method), len(yc), iptr(ym),
+                                               iptr(yc), float(energy), dptr(cc), cfg.size, dptr(cfg), dg.size,
+                                               dptr(dg), dptr(vals), dptr(errs), dptr(cf), dptr(dens)),
+               "ecg_expectation_values")
+        cf, dens = cf[:, :cfg.size], dens[:, :dg.size]
+        if raw:
+            return vals, errs, cf, dens
+        out = expc.unpack(vals, errs, n)
+        if cfg.size:
+            out["cf"] = cf
+        if dg.size:
+            out["dens"] = dens
+        return out
+
+    def expectation_values_g(self, nbasis, which=1, method=1, cf_grid=None, dens_grid=None):
+        """ExpectationValuesG (src/workproc.f90:7785-8366) for a 'G'
+        context: ComputeMatElem(1, nbasis), the which-th eigenpair (ZHEGVX
+        semantics, c^H S c = 1), then the expectation-value pass with
+        Glob_CurrEnergy = that eigenvalue.  Returns the dict of
+        expectation_values with "E" added."""
+        E, err, _ = self.energy_ga(1, nbasis, which=which, want_vector=True)
+        if err != 0:
+            raise EcgError(err, "ExpectationValuesG eigenproblem")
+        out = self.expectation_values(nbasis, E, None, method, cf_grid, dens_grid)
+        out["E"] = E
+        return out
 
     def eval_candidates(self, nbase, candidates, approx_energy, tol, max_iter=20):
         """The BasisEnlI trial loop (src/workproc.f90:4054-4070) for a batch:

@@ -16,7 +16,7 @@ import re
 
 import numpy as np
 
-__all__ = ["System", "transposition_matrix", "expand_yhy", "parse_young"]
+__all__ = ["System", "transposition_matrix", "expand_y", "expand_yhy", "parse_young"]
 
 _ALLOWED = set("0123456789P+-*()")
 
@@ -95,25 +95,36 @@ def _collect(terms):
     return [(c, m) for c, m in acc.values() if c != 0]
 
 
+def _factor_matrix(perms, npart, reverse=False):
+    m = np.eye(npart - 1, dtype=np.int64)
+    seq = perms if not reverse else perms[::-1]
+    for p, q in seq:
+        m = transposition_matrix(p, q, npart) @ m
+    return m
+
+
+def expand_y(expr, npart):
+    """Expand Y itself into (coefficient, matrix) terms with identical
+    matrices merged: Glob_YMatr / Glob_YCoeff (src/workproc.f90:920-1048),
+    the last factor first, then right-multiplied by factors m-1 .. 1."""
+    factors = parse_young(expr)
+    terms = _collect([(c, _factor_matrix(pp, npart)) for c, pp in factors[-1]])
+    for f in reversed(factors[:-1]):
+        terms = _collect([(cs * ck, ms @ _factor_matrix(pk, npart)) for ck, pk in f for cs, ms in terms])
+    return terms
+
+
 def expand_yhy(expr, npart):
     """Expand Y^+Y into (coefficient, matrix) terms with identical matrices
     merged, in the order the reference produces them
     (src/workproc.f90:920-1202).  A product of permutation operators acts on
     the parameter matrices as the reversed product of their matrices."""
     factors = parse_young(expr)
-    n = npart - 1
 
     def mat(perms, reverse=False):
-        m = np.eye(n, dtype=np.int64)
-        seq = perms if not reverse else perms[::-1]
-        for p, q in seq:
-            m = transposition_matrix(p, q, npart) @ m
-        return m
+        return _factor_matrix(perms, npart, reverse)
 
-    # Y: the last factor first, then right-multiply by factors m-1 .. 1
-    terms = _collect([(c, mat(pp)) for c, pp in factors[-1]])
-    for f in reversed(factors[:-1]):
-        terms = _collect([(cs * ck, ms @ mat(pk)) for ck, pk in f for cs, ms in terms])
+    terms = expand_y(expr, npart)
     # Y^+Y: right-multiply by the reversed factors 1 .. m
     for f in factors:
         terms = _collect([(cs * ck, ms @ mat(pk, reverse=True)) for ck, pk in f for cs, ms in terms])
@@ -140,6 +151,9 @@ class System:
         self.yhy_coeffs = np.array([c for c, _ in terms], dtype=np.int32)
         self.yhy_mats = np.array([mm for _, mm in terms], dtype=np.int32)
         self.T = len(terms)
+        yterms = expand_y(symmetry, self.npart)
+        self.y_coeffs = np.array([c for c, _ in yterms], dtype=np.int32)
+        self.y_mats = np.array([mm for _, mm in yterms], dtype=np.int32)
 
     @property
     def mass_matrix_cm(self):
@@ -149,6 +163,11 @@ class System:
     def yhy_mats_cm(self):
         """Glob_YHYMatr(n, n, T) flattened column-major."""
         return np.ascontiguousarray(np.transpose(self.yhy_mats, (0, 2, 1))).ravel()
+
+    @property
+    def y_mats_cm(self):
+        """Glob_YMatr(n, n, NumYTerms) flattened column-major."""
+        return np.ascontiguousarray(np.transpose(self.y_mats, (0, 2, 1))).ravel()
 
     def __repr__(self):
         return f"System(n={self.n}, T={self.T}, symmetry={self.symmetry!r})"

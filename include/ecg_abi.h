@@ -145,6 +145,31 @@ int ecg_energy_ga(ecg_ctx* ctx, int nmin, int nmax, int mat_elem_needed, int whi
 int ecg_energy_gb_adjoint(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, int which, double* energy,
                           double* grad_host);
 
+/* The expectation-value pass of ExpectationValuesG, src/workproc.f90:
+ * 8159-8366, with MatrixElementsForExpcVals (src/matelem.f90:949-1983) for
+ * every pair of functions 1..nbasis and every symmetry term:
+ *   symm_adapt_method 1: Y^+Y (the context's terms) on the ket; the error
+ *                        bound adds 2|beta| per term;
+ *   symm_adapt_method 2: Y on bra and ket, all (k, kk) pairs of the ny
+ *                        terms y_mats_host (n x n x ny, Glob_YMatr) with
+ *                        coefficients y_coeffs_host (Glob_YCoeff); 3|beta|.
+ * masses_host = Glob_Mass (m0, m1..mn); energy = Glob_CurrEnergy (the
+ * eigenvalue, used by the Drachmanised terms); c_host = the eigenvector
+ * (nbasis complex), or NULL for Glob_c (left there by ecg_energy_ga with
+ * want_vector).  Glob_diagS must hold functions 1..nbasis (any
+ * ComputeMatElem(1, nbasis) has set it).
+ * Outputs (NULL to skip): values_host / errors_host, 6np + 9 each in the
+ * MEkl order of src/workproc.f90:8045-8060: 1/r^2, 1/r, r, r^2, delta(r),
+ * Drachmanised delta(r) (np each, vech order (1,1),(1,2)..(n,n)), then H,
+ * S, T, V, MV, drach_MV, Darwin, drach_Darwin, OO; errors_host are the
+ * MEkl_e bounds (already times epsilon).  cf_host (np x ncf) and dens_host
+ * ((n+1) x ndens): correlation functions on cf_grid_host and particle
+ * densities on dens_grid_host (ncf / ndens may be 0). */
+int ecg_expectation_values(ecg_ctx* ctx, int nbasis, const double* masses_host, int symm_adapt_method, int ny,
+                           const int* y_mats_host, const int* y_coeffs_host, double energy, const double* c_host,
+                           int ncf, const double* cf_grid_host, int ndens, const double* dens_grid_host,
+                           double* values_host, double* errors_host, double* cf_host, double* dens_host);
+
 /* Device -> host copies of the context arrays (any pointer may be NULL).
  * H_host, S_host: n x n with leading dimension ld_host. */
 int ecg_get_matrices(ecg_ctx* ctx, int n, double* H_host, double* S_host, int ld_host, double* diagS_host,

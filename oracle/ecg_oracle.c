@@ -41,21 +41,15 @@
 #include <omp.h>
 #endif
 
-#define NN 5                  /* Glob_MaxAllowedNumOfPseudoParticles */
-#define NNP (NN * (NN + 1) / 2)
-#define TMAX 720              /* 6! terms is the largest symmetric group here */
-
-typedef double complex cplx;
+#include "ecg_oracle.h"
 
 /* ---- module globals (the subset of src/globvars.f90 the path reads) ---- */
-static int g_n, g_np, g_npt, g_T;
-static double g_mass[NN][NN];      /* Glob_MassMatrix(i,j) -> g_mass[i][j] */
-static double g_q0, g_q[NN];       /* Glob_PseudoCharge0, Glob_PseudoCharge */
-static int g_P[TMAX][NN][NN];      /* Glob_YHYMatr(i,j,t) -> g_P[t][i][j] */
-static int g_coef[TMAX];           /* Glob_YHYCoeff */
-static double g_2r3n2;             /* Glob_2raised3n2 = 2^(3n/2) */
-
-static const double SQRTPI = 1.77245385090551602729816748334115;
+int g_n, g_np, g_npt, g_T;
+double g_mass[NN][NN];             /* Glob_MassMatrix(i,j) -> g_mass[i][j] */
+double g_q0, g_q[NN];              /* Glob_PseudoCharge0, Glob_PseudoCharge */
+int g_P[TMAX][NN][NN];             /* Glob_YHYMatr(i,j,t) -> g_P[t][i][j] */
+int g_coef[TMAX];                  /* Glob_YHYCoeff */
+double g_2r3n2;                    /* Glob_2raised3n2 = 2^(3n/2) */
 
 /* Set the system.  mass_cm is the n x n mass matrix column-major,
  * charges = (q0, q1..qn), yhy_cm = T column-major n x n integer matrices. */

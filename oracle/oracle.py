@@ -6,7 +6,9 @@ The product (libecgb200.so and the ecg_b200 package) never imports this.
 
 The glue functions below restate EnergyIA / EnergyIAM / EnergyIB
 (src/workproc.f90:1954-2154) on top of the C restatements of
-ComputeMatElem(AndDeriv), GHEPIIS and the gradient contraction.
+ComputeMatElem(AndDeriv), GHEPIIS and the gradient contraction, and the
+term list of ExpectationValuesG (src/workproc.f90:8175-8347) on top of the
+C restatement of its accumulation loop.
 """
 import ctypes as C
 import os
@@ -48,6 +50,13 @@ def load():
                                     C.c_double, _dp, C.c_int, C.c_int, _dp, _ip]
         lib.orc_ghepiis.restype = C.c_int
         lib.orc_gradient_contract.argtypes = [C.c_int, C.c_int, C.c_int, _dp, C.c_int, _dp, C.c_double, _dp]
+        lib.orc_set_masses.argtypes = [_dp]
+        lib.orc_expc_matrix_elements.argtypes = [_dp, _dp, _ip, _ip, C.c_double, _dp, C.c_int, _dp, _dp, C.c_int,
+                                                 _dp, _dp]
+        lib.orc_expectation_values.argtypes = [_dp, C.c_int, _dp, _dp, C.c_int, _ip, _ip, _dp, _dp, C.c_int,
+                                               C.c_double, C.c_int, _dp, C.c_int, _dp, _dp, _dp, _dp, _dp]
+        lib.orc_set_masses_ld.argtypes = [_dp]
+        lib.orc_expectation_values_ld.argtypes = lib.orc_expectation_values.argtypes
         lib.orc_set_threads.argtypes = [C.c_int]
         lib.orc_get_threads.restype = C.c_int
         _lib = lib
@@ -156,6 +165,59 @@ class Oracle:
         g = np.zeros(nfo * self.npt)
         self.lib.orc_gradient_contract(nfo, nfa, nfru, _p(self.D), self.D.shape[1], _p(self.c), E, _p(g))
         return E, g, err, it
+
+    # ExpectationValuesG term lists, src/workproc.f90:8175-8347
+    def expc_terms(self, method):
+        """(Pbra, Pket, coef1, coef2, err_mult) for SymmAdaptMethod 1
+        (identity bra, Y^+Y_t ket, YHYCoeff_t) or 2 (Y_k bra, Y_kk ket,
+        YCoeff_k YCoeff_kk; k outer, kk inner)."""
+        n, sysm = self.n, self.sys
+        if method == 1:
+            pb = [np.eye(n, dtype=np.int32)] * sysm.T
+            pk = list(sysm.yhy_mats)
+            c1 = [float(c) for c in sysm.yhy_coeffs]
+            c2 = [1.0] * sysm.T
+            em = 2
+        elif method == 2:
+            ny = len(sysm.y_coeffs)
+            pb = [sysm.y_mats[k] for k in range(ny) for kk in range(ny)]
+            pk = [sysm.y_mats[kk] for k in range(ny) for kk in range(ny)]
+            c1 = [float(sysm.y_coeffs[k]) for k in range(ny) for kk in range(ny)]
+            c2 = [float(sysm.y_coeffs[kk]) for k in range(ny) for kk in range(ny)]
+            em = 3
+        else:
+            raise ValueError("SymmAdaptMethod is 1 or 2")
+
+        def cm(mats):
+            return np.ascontiguousarray(np.array([np.asarray(m).T for m in mats], dtype=np.int32)).ravel()
+        return cm(pb), cm(pk), np.array(c1), np.array(c2), em
+
+    def expectation_values(self, K, c, curr_energy, method=1, cf_grid=None, dens_grid=None, diagS=None,
+                           extended=False):
+        """The accumulation loop of ExpectationValuesG over functions 1..K
+        with eigenvector c and Glob_CurrEnergy = curr_energy.  diagS defaults
+        to this oracle's (set by compute_mat_elem).  Returns (sums, errs, cf,
+        dens): 6np+9 values and error estimates in the MEkl order, cf np x
+        ncf, dens (n+1) x ndens.  extended=True evaluates the same source in
+        x87 extended precision (a more accurate value of the same sums)."""
+        self.activate()
+        m = np.ascontiguousarray(self.sys.masses, dtype=np.float64)
+        (self.lib.orc_set_masses_ld if extended else self.lib.orc_set_masses)(_p(m))
+        fn = self.lib.orc_expectation_values_ld if extended else self.lib.orc_expectation_values
+        pb, pk, c1, c2, em = self.expc_terms(method)
+        nt = len(c1)
+        cf_grid = np.ascontiguousarray(cf_grid if cf_grid is not None else np.zeros(0), dtype=np.float64)
+        dens_grid = np.ascontiguousarray(dens_grid if dens_grid is not None else np.zeros(0), dtype=np.float64)
+        nv = 6 * self.np + 9
+        sums, errs = np.zeros(nv), np.zeros(nv)
+        cf = np.zeros((self.np, max(cf_grid.size, 1)), order="F")
+        dens = np.zeros((self.n + 1, max(dens_grid.size, 1)), order="F")
+        cc = np.ascontiguousarray(c[:K], dtype=np.complex128)
+        dS = np.ascontiguousarray((self.diagS if diagS is None else diagS)[:K], dtype=np.float64)
+        fn(_p(self.params), K, _p(cc), _p(dS), nt, pb.ctypes.data_as(_ip), pk.ctypes.data_as(_ip), _p(c1), _p(c2),
+           em, curr_energy, cf_grid.size, _p(cf_grid), dens_grid.size, _p(dens_grid), _p(sums), _p(errs), _p(cf),
+           _p(dens))
+        return sums, errs, cf[:, :cf_grid.size], dens[:, :dens_grid.size]
 
     # BasisEnlI trial loop, src/workproc.f90:4054-4070
     def trial_loop(self, nbase, candidates, approx_e, tol, start, max_iter=20):
