@@ -16,9 +16,12 @@
 // u_P = e_a (a = b) or e_a - e_b, d_P = C^-1 u_P and TrCJ_P = u_P' C^-1 u_P;
 // then tr[C^-1 X C^-1 J_P] = d_P' X d_P, which is what the reference's
 // ME_rXr_over_rij / ME_rXr_rYr_over_rij (src/matelem.f90:753-945) sum
-// element by element.  The mass-velocity products of rank-one matrices
-// (J C, C J_ii C, src/matelem.f90:1487-1597) are taken as outer products.
-// Results agree with the reference's to rounding.
+// element by element.  Most matrices the reference builds for these traces
+// are rank one or sums of rank-one terms (J C, C J_ii C in the
+// mass-velocity terms, the Wc1..Wc3 of the orbit-orbit loops, E_ii / E_jj
+// and the all-ones matrix of the Drachmanised Darwin term), so their traces
+// are taken as dot products.  Results agree with the reference's to
+// rounding.
 //
 // TrCJCJ(i,j,p,q) of src/matelem.f90:1270-1300 is never assigned for
 // i = j < p < q (n >= 3) but is read by the 1/(r_ij r_pq) loop; the
@@ -100,6 +103,26 @@ __device__ __forceinline__ cd dot(const cd (&u)[N], const cd (&v)[N])
     return s;
 }
 
+// v[k] for a runtime k, by selects (keeps v in registers)
+template <int N>
+__device__ __forceinline__ cd pick(const cd (&v)[N], int k)
+{
+    cd r = v[0];
+#pragma unroll
+    for (int m = 1; m < N; m++)
+        if (k == m) r = v[m];
+    return r;
+}
+template <int N>
+__device__ __forceinline__ double pickd(const double (&v)[N], int k)
+{
+    double r = v[0];
+#pragma unroll
+    for (int m = 1; m < N; m++)
+        if (k == m) r = v[m];
+    return r;
+}
+
 // Per pair index P = (a, b) in vech order: d_P = C^-1 u_P and TrCJ_P.
 template <int N>
 struct PairVecs {
@@ -127,85 +150,6 @@ __device__ __forceinline__ void pair_vecs(const cd (&inv)[N][N], PairVecs<N>& pv
                 pv.tr[P] = inv[a][a] + inv[b][b] - inv[b][a] - inv[b][a];
             }
         }
-}
-
-// <phi_k| r'Xr / r_P |phi_l> (ME_rXr_over_rij, src/matelem.f90:753-818)
-template <int N>
-__device__ __forceinline__ cd rxr_over(const cd (&X)[N][N], const cd (&inv)[N][N], const cd (&d)[N], cd me1, cd trcj)
-{
-    const cd trcx = trmm(inv, X);
-    const cd t = quad(d, X, d);
-    return me1 * (0.5 * (3.0 * trcx - cdiv(t, trcj)));
-}
-
-// <phi_k| (r'Xr)(r'Yr) / r_P |phi_l> (ME_rXr_rYr_over_rij,
-// src/matelem.f90:821-945) with Xs, Ys the symmetric parts.
-template <int N>
-__device__ __forceinline__ cd rxr_ryr_over(const cd (&X)[N][N], const cd (&Y)[N][N], const cd (&inv)[N][N],
-                                           const cd (&d)[N], cd me1, cd trcj)
-{
-    cd Xs[N][N], Ys[N][N];
-#pragma unroll
-    for (int p = 0; p < N; p++) {
-        Xs[p][p] = X[p][p];
-        Ys[p][p] = Y[p][p];
-#pragma unroll
-        for (int q = p + 1; q < N; q++) {
-            Xs[p][q] = 0.5 * (X[p][q] + X[q][p]);
-            Xs[q][p] = Xs[p][q];
-            Ys[p][q] = 0.5 * (Y[p][q] + Y[q][p]);
-            Ys[q][p] = Ys[p][q];
-        }
-    }
-    cd CX[N][N], CY[N][N];
-    mm(inv, Xs, CX);
-    mm(inv, Ys, CY);
-    const cd trcx = trace(CX), trcy = trace(CY), trcxcy = trmm(CX, CY);
-    cd e[N], f[N];
-#pragma unroll
-    for (int p = 0; p < N; p++) {
-        cd se = mk(0.0, 0.0), sf = mk(0.0, 0.0);
-#pragma unroll
-        for (int q = 0; q < N; q++) {
-            se = cfma(Xs[p][q], d[q], se);
-            sf = cfma(Ys[p][q], d[q], sf);
-        }
-        e[p] = se;
-        f[p] = sf;
-    }
-    const cd txj = dot(d, e), tyj = dot(d, f);
-    cd g[N];
-#pragma unroll
-    for (int p = 0; p < N; p++) {
-        cd s = mk(0.0, 0.0);
-#pragma unroll
-        for (int q = 0; q < N; q++) s = cfma(inv[p][q], f[q], s);
-        g[p] = s;
-    }
-    const cd txyj = dot(e, g);
-    const cd r = 9.0 * (trcy * trcx) + 6.0 * trcxcy - cdiv(3.0 * (trcy * txj + trcx * tyj) + 4.0 * txyj, trcj) +
-                 cdiv(3.0 * (txj * tyj), trcj * trcj);
-    return me1 * (0.25 * r);
-}
-
-// ME_dXd_dYd, src/matelem.f90:1998-2016
-template <int N>
-__device__ __forceinline__ cd dxd_dyd(const cd (&X)[N][N], const cd (&Y)[N][N], const cd (&inv)[N][N],
-                                      const cd (&tCk)[N][N], const cd (&tCl)[N][N], cd S)
-{
-    cd T1[N][N], T2[N][N], M[N][N], MM[N][N];
-    const cd tr1 = trmm(X, tCk);
-    const cd tr2 = trmm(tCl, Y);
-    mm(X, tCk, T1);
-    mm(tCk, T1, T2);
-    mm(inv, T2, M);
-    const cd tr3 = trace(M);
-    mm(Y, tCl, T1);
-    mm(tCl, T1, T2);
-    mm(inv, T2, MM);
-    const cd tr4 = trace(MM);
-    const cd tr5 = trmm(M, MM);
-    return (36.0 * (tr3 * tr4) + 24.0 * tr5 - 36.0 * (tr1 * tr4) - 36.0 * (tr2 * tr3) + 36.0 * (tr1 * tr2)) * S;
 }
 
 // tCl X tCl and tr(tCl X) (the products of ME_dXd / ME_dXd_over_rij)
@@ -386,24 +330,26 @@ __device__ __forceinline__ void term_matrices(const double (&Ak)[N][N], const do
         for (int j = 0; j < N; j++) tCl[i][j] = mk(R1[i][j], R2[i][j]);
 }
 
-// 1/(r_P r_Q) for pair indices P before Q in vech order (src/matelem.f90:
-// 1302-1339); TrCJCJ is the square of u_Q' C^-1 u_P, zero where the
-// reference leaves it unassigned (P = (a,a), Q = (c,d), a < c < d).
+// 1/(r_P r_Q) for pair indices P = (a,b) before Q = (c,d) in vech order
+// (src/matelem.f90:1302-1339), from dP = C^-1 u_P and the two TrCJ:
+// TrCJCJ is the square of u_Q' C^-1 u_P, zero where the reference leaves it
+// unassigned (a = b < c < d).
 template <int N>
-__device__ __forceinline__ cd pair_pair(const PairVecs<N>& pv, int P, int a, int b, int Q, int c, int d, cd S)
+__device__ __forceinline__ cd pair_pair(const cd (&dP)[N], cd trP, cd trQ, bool same, int a, int b, int c, int d,
+                                        cd S)
 {
     const cd cnumb = (4.0 / PI_D) * S;
-    if (P == Q) return cdiv(2.0 * S, pv.tr[P]);
+    if (same) return cdiv(2.0 * S, trP);
     cd x;
-    if (a == b && c != d)
-        x = (a < c) ? mk(0.0, 0.0) : pv.d[Q][a];  // a < c < d unassigned; else inv(a,c) - inv(a,d)
-    else if (c == d)
-        x = pv.d[P][c];
+    if (c == d)
+        x = pick(dP, c);
+    else if (a == b && a < c)
+        x = mk(0.0, 0.0);
     else
-        x = pv.d[P][c] - pv.d[P][d];
+        x = pick(dP, c) - pick(dP, d);
     const cd tt = x * x;
     const cd caux = csqrt(tt);
-    const cd sq = csqrt(pv.tr[P] * pv.tr[Q]);
+    const cd sq = csqrt(trP * trQ);
     if (caux.x != 0.0 || caux.y != 0.0) {
         const cd caux1 = cdiv(caux, sq);
         const cd w = mk(1.0, 0.0) - caux1 * caux1;
@@ -414,20 +360,53 @@ __device__ __forceinline__ cd pair_pair(const PairVecs<N>& pv, int P, int a, int
     return cdiv(cnumb, sq);
 }
 
+// (a, b) of vech index P, a <= b
 template <int N>
+__device__ __forceinline__ void vech_pair(int P, int& a, int& b)
+{
+    a = 0;
+    while (P >= N - a) {
+        P -= N - a;
+        a++;
+    }
+    b = a + P;
+}
+
+// The pass is split into four kernels by the values they produce, each
+// recomputing the short common part (matrices, inverse, overlap): 0 = T, V,
+// H, S, the pair quantities and Darwin; 1 = orbit-orbit; 2 = mass-velocity
+// and its Drachmanised form; 3 = Drachmanised Darwin.  Smaller kernels keep
+// their code in the instruction cache and their matrices in registers.
+constexpr int EXPC_SECTIONS = 4;
+
+// values of section SEC (local index order), and local -> MEkl index
+template <int N, int SEC>
+__host__ __device__ constexpr int sec_nv()
+{
+    return SEC == 0 ? 6 * (N * (N + 1) / 2) + 5 : (SEC == 2 ? 2 : 1);
+}
+template <int N, int SEC>
+__device__ __forceinline__ int sec_global(int l)
+{
+    constexpr int B = 6 * (N * (N + 1) / 2);
+    if (SEC == 0) return l < B + 4 ? l : B + 6;  // ..., H, S, T, V, then Darwin
+    if (SEC == 1) return B + 8;                   // OO
+    if (SEC == 2) return B + 4 + l;               // MV, drach_MV
+    return B + 7;                                 // drach_Darwin
+}
+
+template <int N, int SEC>
 __global__ void __launch_bounds__(EXPC_BLK) k_expc(const double* __restrict__ params, int npt,
                                                    const cd* __restrict__ cvec, const double* __restrict__ diagS,
                                                    const double* __restrict__ terms, ExpcArgs ea,
                                                    double* __restrict__ partial)
 {
     constexpr int NP = N * (N + 1) / 2;
+    constexpr int nvs = sec_nv<N, SEC>();
     extern __shared__ double sacc[];
     const int tid = threadIdx.x;
     const int nv = ea.nv;
-    for (int a = 0; a < nv; a++) {
-        sacc[a * EXPC_BLK + tid] = 0.0;
-        sacc[(nv + a) * EXPC_BLK + tid] = 0.0;
-    }
+    for (int a = 0; a < 2 * nvs; a++) sacc[a * EXPC_BLK + tid] = 0.0;
     const SysParams& sp = ea.sp;
     const double(&mass)[NMAX + 1] = ea.mass;
     for (long long pidx = (long long)blockIdx.x * EXPC_BLK + tid; pidx < ea.npairs;
@@ -442,7 +421,7 @@ __global__ void __launch_bounds__(EXPC_BLK) k_expc(const double* __restrict__ pa
         const double factor = (pi == pj) ? 1.0 / sqrt(diagS[pi] * diagS[pi]) : 2.0 / sqrt(diagS[pi] * diagS[pj]);
         Acc acc;
         acc.s = sacc + tid;
-        acc.e = sacc + nv * EXPC_BLK + tid;
+        acc.e = sacc + nvs * EXPC_BLK + tid;
         acc.rci = ci.x; acc.ici = ci.y; acc.rcj = cj.x; acc.icj = cj.y;
         acc.p1 = ci.x * cj.x + ci.y * cj.y;
         acc.p2 = ci.y * cj.x - ci.x * cj.y;
@@ -459,7 +438,14 @@ __global__ void __launch_bounds__(EXPC_BLK) k_expc(const double* __restrict__ pa
             inverse_overlap<N>(tCkl, absdet, sp.two_r3n2, inv, S);
             PairVecs<N> pv;
             pair_vecs<N>(inv, pv);
+            cd rm[NP];  // <1/r_P>
+            if constexpr (SEC != 0) {
+                const cd cn = TWO_OVER_SQRTPI * S;
+#pragma unroll
+                for (int P = 0; P < NP; P++) rm[P] = cdiv(cn, csqrt(pv.tr[P]));
+            }
 
+            if constexpr (SEC == 0) {
             // kinetic energy, src/matelem.f90:1203-1229
             cd T;
             {
@@ -474,7 +460,6 @@ __global__ void __launch_bounds__(EXPC_BLK) k_expc(const double* __restrict__ pa
                 T = 6.0 * (S * tr);
             }
             // 1/r, r, r^2, delta(r), V, src/matelem.f90:1231-1268
-            cd rm[NP];
             cd V = mk(0.0, 0.0), V0 = mk(0.0, 0.0);
             {
                 const cd cn = TWO_OVER_SQRTPI * S;
@@ -526,7 +511,7 @@ __global__ void __launch_bounds__(EXPC_BLK) k_expc(const double* __restrict__ pa
                             dw = rfma(f, dr, dw);
                         }
                     }
-                acc.add(6 * NP + 6, (-0.5 * PI_D) * dw);
+                acc.add(6 * NP + 4, (-0.5 * PI_D) * dw);
             }
 
             // Drachmanised delta(r_P), src/matelem.f90:1349-1392
@@ -534,25 +519,46 @@ __global__ void __launch_bounds__(EXPC_BLK) k_expc(const double* __restrict__ pa
                 cd sumq[NP];
 #pragma unroll
                 for (int P = 0; P < NP; P++) sumq[P] = mk(0.0, 0.0);
-                int P = 0;
+                // charge weights per pair index, q0 q_a or q_a q_b
+                double wq[NP];
+                {
+                    int P = 0;
 #pragma unroll
-                for (int a = 0; a < N; a++)
+                    for (int a = 0; a < N; a++)
 #pragma unroll
-                    for (int b = a; b < N; b++, P++) {
-                        const double wP = (a == b) ? sp.q0 * sp.q[a] : sp.q[a] * sp.q[b];
-                        int Q = P;
+                        for (int b = a; b < N; b++, P++) wq[P] = (a == b) ? sp.q0 * sp.q[a] : sp.q[a] * sp.q[b];
+                }
+                // one loop over the pairs (P, Q >= P); each R adds to both
+                // sums, so every sum runs over Q in ascending order
+#pragma unroll 1
+                for (int P = 0; P < NP; P++) {
+                    int a, b;
+                    vech_pair<N>(P, a, b);
+                    cd dP[N];
 #pragma unroll
-                        for (int c = a; c < N; c++)
+                    for (int m = 0; m < N; m++) {
+                        cd r = pv.d[0][m];
 #pragma unroll
-                            for (int d = c; d < N; d++) {
-                                if (c == a && d < b) continue;
-                                const double wQ = (c == d) ? sp.q0 * sp.q[c] : sp.q[c] * sp.q[d];
-                                const cd R = pair_pair<N>(pv, P, a, b, Q, c, d, S);
-                                sumq[P] = rfma(wQ, R, sumq[P]);
-                                if (Q != P) sumq[Q] = rfma(wP, R, sumq[Q]);
-                                Q++;
-                            }
+                        for (int X = 1; X < NP; X++)
+                            if (X == P) r = pv.d[X][m];
+                        dP[m] = r;
                     }
+                    const cd trP = pick(pv.tr, P);
+                    const double wP = pickd(wq, P);
+#pragma unroll 1
+                    for (int Q = P; Q < NP; Q++) {
+                        int c, d;
+                        vech_pair<N>(Q, c, d);
+                        const cd R = pair_pair<N>(dP, trP, pick(pv.tr, Q), Q == P, a, b, c, d, S);
+                        const double wQ = pickd(wq, Q);
+#pragma unroll
+                        for (int X = 0; X < NP; X++) {
+                            if (X == P) sumq[X] = rfma(wQ, R, sumq[X]);
+                            if (X == Q && Q != P) sumq[X] = rfma(wP, R, sumq[X]);
+                        }
+                    }
+                }
+                int P = 0;
                 cd W1[N][N], W2[N][N], Mc[N][N];
 #pragma unroll
                 for (int i = 0; i < N; i++)
@@ -577,77 +583,107 @@ __global__ void __launch_bounds__(EXPC_BLK) k_expc(const double* __restrict__ pa
                     }
             }
 
-            // orbit-orbit, src/matelem.f90:1394-1485
-            {
-                cd oo1 = mk(0.0, 0.0), oo2 = mk(0.0, 0.0);
-#pragma unroll
-                for (int i = 0; i < N; i++)
-#pragma unroll
-                    for (int j = 0; j < N; j++) {
-                        const int Pj = vech_index(N, j, j);
-                        cd W1[N][N], W2[N][N], W3[N][N];
-                        const cd tr1 = tCl[j][i];
-                        const cd tr3 = 3.0 * tCl[j][j];
-#pragma unroll
-                        for (int p = 0; p < N; p++)
-#pragma unroll
-                            for (int q = 0; q < N; q++) {
-                                W1[q][p] = tCl[q][i] * tCl[p][j] + tCl[q][j] * tCl[p][i];
-                                W2[p][q] = tCkl[p][j] * tCl[q][j];
-                                W3[q][p] = mk(0.0, 0.0);
-                            }
-#pragma unroll
-                        for (int p = 0; p < N; p++) W1[p][j] = W1[p][j] + tCkl[p][j] * tCl[j][i];
-#pragma unroll
-                        for (int p = 0; p < N; p++) {
-                            W1[j][p] = W1[j][p] + tCl[i][j] * tCl[p][j] + tr3 * tCl[p][i];
-                            W3[j][p] = tCl[p][i];
-                        }
-                        const cd cnumb = rxr_over(W1, inv, pv.d[Pj], rm[Pj], pv.tr[Pj]);
-                        const cd ctemp = rxr_ryr_over(W2, W3, inv, pv.d[Pj], rm[Pj], pv.tr[Pj]);
-                        const cd caux = -6.0 * ((tr1 + tr1) * rm[Pj]) + 4.0 * cnumb - 8.0 * ctemp;
-                        oo1 = oo1 - (sp.q[j] / mass[j + 1]) * caux;
-                    }
-                oo1 = (sp.q0 / mass[0]) * oo1;
-#pragma unroll
-                for (int i = 0; i < N; i++)
-#pragma unroll
-                    for (int j = 0; j < N; j++) {
-                        if (j <= i) continue;
-                        const int Pij = vech_index(N, i, j);
-                        cd W1[N][N], W2[N][N], W3[N][N];
-                        const cd tr1 = tCl[j][i];
-                        const cd tr3 = 3.0 * tCl[j][j];
-#pragma unroll
-                        for (int p = 0; p < N; p++)
-#pragma unroll
-                            for (int q = 0; q < N; q++) {
-                                W1[q][p] = tCl[q][i] * tCl[p][j] + tCl[q][j] * tCl[p][i];
-                                W2[p][q] = tCkl[p][j] * tCl[q][j];
-                                W3[q][p] = mk(0.0, 0.0);
-                            }
-#pragma unroll
-                        for (int p = 0; p < N; p++) {
-                            const cd t = tCkl[p][j] * tCl[j][i];
-                            W1[p][j] = W1[p][j] + t;
-                            W1[p][i] = W1[p][i] - t;
-                        }
-#pragma unroll
-                        for (int p = 0; p < N; p++) {
-                            const cd cn = tCl[i][j] * tCl[p][j] + tr3 * tCl[p][i];
-                            W1[j][p] = W1[j][p] + cn;
-                            W1[i][p] = W1[i][p] - cn;
-                            W3[j][p] = tCl[p][i];
-                            W3[i][p] = -tCl[p][i];
-                        }
-                        const cd cnumb = rxr_over(W1, inv, pv.d[Pij], rm[Pij], pv.tr[Pij]);
-                        const cd ctemp = rxr_ryr_over(W2, W3, inv, pv.d[Pij], rm[Pij], pv.tr[Pij]);
-                        const cd caux = -6.0 * ((tr1 + tr1) * rm[Pij]) + 4.0 * cnumb - 8.0 * ctemp;
-                        oo2 = oo2 + (sp.q[i] * sp.q[j] / (mass[i + 1] * mass[j + 1])) * caux;
-                    }
-                acc.add(6 * NP + 8, 0.5 * (oo1 + oo2));
             }
 
+            if constexpr (SEC == 1) {
+            // orbit-orbit, src/matelem.f90:1394-1485
+            // Each iteration's matrices are rank one or sums of rank-one
+            // terms: Wc2 = x y', Wc3 = u z' and Wc1 = z y' + y z' + t x u'
+            // + u v' with x = tCkl(:,j), y = tCl(:,j), z = tCl(:,i),
+            // t = tCl(j,i), v = tCl(i,j) y + 3 tCl(j,j) z, u = e_j (first
+            // loop) or e_j - e_i (second loop), so the traces of
+            // ME_rXr_over_rij / ME_rXr_rYr_over_rij reduce to dot products
+            // with C^-1 u, C^-1 x and C^-1 z.  The iterations run as one
+            // loop; columns are picked with selects, so the matrices stay in
+            // registers.
+            {
+                const cd cn = TWO_OVER_SQRTPI * S;
+                double qv[N], mv[N];
+#pragma unroll
+                for (int p = 0; p < N; p++) {
+                    qv[p] = sp.q[p];
+                    mv[p] = mass[p + 1];
+                }
+                cd oo1 = mk(0.0, 0.0), oo2 = mk(0.0, 0.0);
+#pragma unroll 1
+                for (int it = 0; it < N * N + N * (N - 1) / 2; it++) {
+                    int i, j;
+                    const bool second = it >= N * N;
+                    if (!second) {
+                        i = it / N;
+                        j = it - i * N;
+                    } else {
+                        int r = it - N * N;
+                        i = 0;
+                        while (r >= N - 1 - i) {
+                            r -= N - 1 - i;
+                            i++;
+                        }
+                        j = i + 1 + r;
+                    }
+                    cd x[N], y[N], z[N], iu[N];
+#pragma unroll
+                    for (int p = 0; p < N; p++) {
+                        x[p] = pick(tCkl[p], j);
+                        y[p] = pick(tCl[p], j);
+                        z[p] = pick(tCl[p], i);
+                        iu[p] = pick(inv[p], j);
+                        if (second) iu[p] = iu[p] - pick(inv[p], i);
+                    }
+                    auto udot = [&](const cd (&w)[N]) -> cd {
+                        cd r = pick(w, j);
+                        if (second) r = r - pick(w, i);
+                        return r;
+                    };
+                    const cd t = pick(z, j);           // tCl(j,i)
+                    const cd tr3 = 3.0 * pick(y, j);   // 3 tCl(j,j)
+                    cd v[N], ix[N], iz[N];
+#pragma unroll
+                    for (int p = 0; p < N; p++) v[p] = t * y[p] + tr3 * z[p];
+#pragma unroll
+                    for (int p = 0; p < N; p++) {
+                        cd a = mk(0.0, 0.0), b = mk(0.0, 0.0);
+#pragma unroll
+                        for (int q = 0; q < N; q++) {
+                            a = cfma(inv[p][q], x[q], a);
+                            b = cfma(inv[p][q], z[q], b);
+                        }
+                        ix[p] = a;
+                        iz[p] = b;
+                    }
+                    // d = C^-1 u_P (up to sign, which cancels) = iu; TrCJ = u' C^-1 u
+                    const cd trcj = udot(iu);
+                    const cd me1 = cdiv(cn, csqrt(trcj));
+                    const cd yiz = dot(y, iz), xiu = dot(x, iu), viu = dot(v, iu), yiu = dot(y, iu);
+                    const cd xiz = dot(x, iz), ziu = dot(z, iu), yix = dot(y, ix);
+                    const cd dx = xiu, dy = yiu, dz = ziu, dv = viu, du = trcj;
+                    // <r'Wc1 r / r_P>
+                    const cd trw = 2.0 * yiz + t * xiu + viu;
+                    const cd dwd = 2.0 * (dz * dy) + t * (dx * du) + du * dv;
+                    const cd cnumb = me1 * (0.5 * (3.0 * trw - cdiv(dwd, trcj)));
+                    // <(r'Wc2 r)(r'Wc3 r) / r_P>
+                    const cd trcx = yix, trcy = ziu;
+                    const cd trcxcy = 0.5 * (yiu * xiz + yiz * xiu);
+                    const cd txj = dx * dy, tyj = du * dz;
+                    const cd txyj = 0.25 * ((dy * dz) * xiu + (dy * du) * xiz + (dx * dz) * yiu + (dx * du) * yiz);
+                    const cd r = 9.0 * (trcy * trcx) + 6.0 * trcxcy -
+                                 cdiv(3.0 * (trcy * txj + trcx * tyj) + 4.0 * txyj, trcj) +
+                                 cdiv(3.0 * (txj * tyj), trcj * trcj);
+                    const cd ctemp = me1 * (0.25 * r);
+                    const cd caux = -6.0 * ((t + t) * me1) + 4.0 * cnumb - 8.0 * ctemp;
+                    const double qj = pickd(qv, j), mj = pickd(mv, j);
+                    if (!second)
+                        oo1 = oo1 - (qj / mj) * caux;
+                    else
+                        oo2 = oo2 + (pickd(qv, i) * qj / (pickd(mv, i) * mj)) * caux;
+                }
+                oo1 = (sp.q0 / mass[0]) * oo1;
+                acc.add(0, 0.5 * (oo1 + oo2));
+            }
+
+            }
+
+            if constexpr (SEC == 2) {
             // mass-velocity, src/matelem.f90:1487-1597: tCk J tCk = s_k s_k',
             // tCk J_ii tCk = tCk(:,i) tCk(i,:) (rank one), so every trace is a
             // quadratic form in C^-1.
@@ -685,7 +721,7 @@ __global__ void __launch_bounds__(EXPC_BLK) k_expc(const double* __restrict__ pa
                     }
                     mv = mv + (1.0 / (mass[i + 1] * mass[i + 1] * mass[i + 1])) * mv_term(a, b, tCk[i][i], tCl[i][i]);
                 }
-                acc.add(6 * NP + 4, (-36.0 / 8.0) * (S * mv));
+                acc.add(0, (-36.0 / 8.0) * (S * mv));
             }
 
             // Drachmanised mass-velocity, src/matelem.f90:1675-1848
@@ -771,10 +807,18 @@ __global__ void __launch_bounds__(EXPC_BLK) k_expc(const double* __restrict__ pa
                     }
                     dmv = dmv + 0.125 * (S * third(a, tCk[k][k], cw));
                 }
-                acc.add(6 * NP + 5, dmv);
+                acc.add(1, dmv);
             }
 
+            }
+
+            if constexpr (SEC == 3) {
             // Drachmanised Darwin, src/matelem.f90:1875-1929
+            // ME_dXd_dYd with X = E_ii, Y = E_jj is rank one on both sides:
+            // tCk E_ii tCk = a a', tCl E_jj tCl = b b' (a = tCk(:,i),
+            // b = tCl(:,j)), so tr3 = a'C^-1 a, tr4 = b'C^-1 b and
+            // tr5 = (a'C^-1 b)^2; with X = ones, tCk X tCk = s s' (s the
+            // column sums of tCk).
             {
                 cd W1[N][N], M3[N][N];
                 const double im0 = 1.0 / (mass[0] * mass[0]);
@@ -785,6 +829,7 @@ __global__ void __launch_bounds__(EXPC_BLK) k_expc(const double* __restrict__ pa
                         W1[p][q] = mk(p == q ? im0 + 1.0 / (mass[p + 1] * mass[p + 1]) : im0, 0.0);
                 const cd trx = clxcl(W1, tCl, M3);  // M3 = tCl W1 tCl, trx = tr(tCl W1)
                 const cd trm = trmm(inv, M3);
+                // first and second terms: E ME_dXd(W1)/4 and the sum of ME_dXd_over_rij(W1)
                 cd dd = 0.25 * (ea.energy * (6.0 * ((trm - trx) * S)));
                 int P = 0;
 #pragma unroll
@@ -792,45 +837,92 @@ __global__ void __launch_bounds__(EXPC_BLK) k_expc(const double* __restrict__ pa
 #pragma unroll
                     for (int b = a; b < N; b++, P++) {
                         const double wq = (a == b) ? sp.q0 * sp.q[a] : sp.q[a] * sp.q[b];
-                        const cd rxr = rxr_over(M3, inv, pv.d[P], rm[P], pv.tr[P]);
+                        const cd rxr = rm[P] * (0.5 * (3.0 * trm - cdiv(quad(pv.d[P], M3, pv.d[P]), pv.tr[P])));
                         dd = dd - (0.25 * wq) * (4.0 * rxr - 6.0 * (trx * rm[P]));
                     }
-                cd X1[N][N], Y1[N][N];
+                // C^-1 tCk and C^-1 tCl
+                cd Vk[N][N], Vl[N][N];
+                mm(inv, tCk, Vk);
+                mm(inv, tCl, Vl);
+                // third term: X = ones, Y = diag((m0 + m_j) / (m0^2 m_j^2))
+                {
+                    cd s[N], is[N];
+                    cd t1 = mk(0.0, 0.0), t2 = mk(0.0, 0.0);
 #pragma unroll
-                for (int p = 0; p < N; p++)
+                    for (int p = 0; p < N; p++) {
+                        cd u = mk(0.0, 0.0), w = mk(0.0, 0.0);
 #pragma unroll
-                    for (int q = 0; q < N; q++) {
-                        X1[p][q] = mk(1.0, 0.0);
-                        Y1[p][q] = mk(p == q ? (mass[0] + mass[p + 1]) / (mass[0] * mass[0] * mass[p + 1] * mass[p + 1])
-                                             : 0.0,
-                                      0.0);
+                        for (int q = 0; q < N; q++) {
+                            u = u + tCk[q][p];
+                            w = w + Vk[p][q];  // (C^-1 tCk 1)_p = (C^-1 s)_p
+                        }
+                        s[p] = u;
+                        is[p] = w;
+                        t1 = t1 + u;
                     }
-                dd = dd + 0.125 * dxd_dyd(X1, Y1, inv, tCk, tCl, S);
+                    cd MM[N][N];  // C^-1 tCl D tCl = Vl D tCl
+                    double w[N];
 #pragma unroll
-                for (int i = 0; i < N; i++)
+                    for (int p = 0; p < N; p++) {
+                        w[p] = (mass[0] + mass[p + 1]) / (mass[0] * mass[0] * mass[p + 1] * mass[p + 1]);
+                        t2 = rfma(w[p], tCl[p][p], t2);
+                    }
+#pragma unroll
+                    for (int p = 0; p < N; p++)
+#pragma unroll
+                        for (int q = 0; q < N; q++) {
+                            cd a = mk(0.0, 0.0);
+#pragma unroll
+                            for (int k = 0; k < N; k++) a = cfma(w[k] * Vl[p][k], tCl[k][q], a);
+                            MM[p][q] = a;
+                        }
+                    const cd t3 = dot(s, is);
+                    const cd t4 = trace(MM);
+                    const cd t5 = quad(s, MM, is);
+                    dd = dd + 0.125 * ((36.0 * (t3 * t4) + 24.0 * t5 - 36.0 * (t1 * t4) - 36.0 * (t2 * t3) +
+                                        36.0 * (t1 * t2)) * S);
+                }
+                // fourth term: pairs i < j with X = E_ii, Y = E_jj
+#pragma unroll
+                for (int i = 0; i < N; i++) {
+                    cd a[N];
+#pragma unroll
+                    for (int p = 0; p < N; p++) a[p] = tCk[p][i];
+                    cd t3 = mk(0.0, 0.0);
+#pragma unroll
+                    for (int p = 0; p < N; p++) t3 = cfma(a[p], Vk[p][i], t3);  // a' C^-1 a
 #pragma unroll
                     for (int j = i + 1; j < N; j++) {
+                        cd t4 = mk(0.0, 0.0), x = mk(0.0, 0.0);
 #pragma unroll
-                        for (int p = 0; p < N; p++)
-#pragma unroll
-                            for (int q = 0; q < N; q++) {
-                                X1[p][q] = mk(p == i && q == i ? 1.0 : 0.0, 0.0);
-                                Y1[p][q] = mk(p == j && q == j ? 1.0 : 0.0, 0.0);
-                            }
+                        for (int p = 0; p < N; p++) {
+                            t4 = cfma(tCl[p][j], Vl[p][j], t4);  // b' C^-1 b
+                            x = cfma(a[p], Vl[p][j], x);         // a' C^-1 b
+                        }
+                        const cd t1 = tCk[i][i], t2 = tCl[j][j];
+                        const cd t5 = x * x;
                         const double cw = (mass[i + 1] + mass[j + 1]) /
                                           (mass[i + 1] * mass[i + 1] * mass[j + 1] * mass[j + 1]);
-                        dd = dd + (0.125 * cw) * dxd_dyd(X1, Y1, inv, tCk, tCl, S);
+                        dd = dd + (0.125 * cw) * ((36.0 * (t3 * t4) + 24.0 * t5 - 36.0 * (t1 * t4) -
+                                                   36.0 * (t2 * t3) + 36.0 * (t1 * t2)) * S);
                     }
-                acc.add(6 * NP + 7, dd);
+                }
+                acc.add(0, dd);
+            }
             }
         }
     }
     __syncthreads();
-    // block sums in a fixed order
-    for (int a = tid; a < 2 * nv; a += EXPC_BLK) {
+    // block sums in a fixed order; the section's slice of partial holds zero
+    // for the values of the other sections
+    double* out = partial + ((size_t)SEC * gridDim.x + blockIdx.x) * 2 * nv;
+    for (int a = tid; a < 2 * nv; a += EXPC_BLK) out[a] = 0.0;
+    __syncthreads();
+    for (int l = tid; l < 2 * nvs; l += EXPC_BLK) {
         double s = 0.0;
-        for (int t = 0; t < EXPC_BLK; t++) s += sacc[a * EXPC_BLK + t];
-        partial[(size_t)blockIdx.x * 2 * nv + a] = s;
+        for (int t = 0; t < EXPC_BLK; t++) s += sacc[l * EXPC_BLK + t];
+        const int li = l < nvs ? l : l - nvs;
+        out[sec_global<N, SEC>(li) + (l < nvs ? 0 : nv)] = s;
     }
 }
 
@@ -942,17 +1034,28 @@ __global__ void k_expc_sum(const double* __restrict__ partial, int nblocks, int 
     out[a] = a >= eps_from ? s * DBL_EPSILON : s;
 }
 
+template <int N, int SEC>
+int launch_sec(Ctx& c, const ExpcArgs& ea, const double* terms, const cd* cvec, double* partial, int nblocks)
+{
+    const size_t smem = (size_t)2 * sec_nv<N, SEC>() * EXPC_BLK * sizeof(double);
+    if (cudaFuncSetAttribute(k_expc<N, SEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return -2;
+    k_expc<N, SEC><<<nblocks, EXPC_BLK, smem, c.stream>>>(c.params, c.npt, cvec, c.diagS, terms, ea, partial);
+    c.launches += 1;
+    return 0;
+}
+
 template <int N>
 int launch_n(Ctx& c, const ExpcArgs& ea, const double* terms, const cd* cvec, const double* cfg, int ncf,
              const double* dg, int ndens, double* partial, int nblocks, double* out, double* gpartial, int gblocks,
              int gchunk, int ngrid, double* gout)
 {
-    const size_t smem = (size_t)2 * ea.nv * EXPC_BLK * sizeof(double);
-    if (cudaFuncSetAttribute(k_expc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (launch_sec<N, 0>(c, ea, terms, cvec, partial, nblocks) || launch_sec<N, 1>(c, ea, terms, cvec, partial, nblocks) ||
+        launch_sec<N, 2>(c, ea, terms, cvec, partial, nblocks) || launch_sec<N, 3>(c, ea, terms, cvec, partial, nblocks))
         return -2;
-    k_expc<N><<<nblocks, EXPC_BLK, smem, c.stream>>>(c.params, c.npt, cvec, c.diagS, terms, ea, partial);
-    k_expc_sum<<<(2 * ea.nv + 127) / 128, 128, 0, c.stream>>>(partial, nblocks, 2 * ea.nv, ea.nv, out);
-    c.launches += 2;
+    k_expc_sum<<<(2 * ea.nv + 127) / 128, 128, 0, c.stream>>>(partial, EXPC_SECTIONS * nblocks, 2 * ea.nv, ea.nv,
+                                                               out);
+    c.launches += 1;
     if (ngrid > 0) {
         const size_t gsm = (size_t)gchunk * EXPC_BLK * sizeof(double);
         if (cudaFuncSetAttribute(k_expc_grid<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm) !=
@@ -1029,7 +1132,7 @@ int expectation_values(Ctx& c, int nbasis, const double* masses, int nterms, con
     };
     const size_t nv = ea.nv;
     if (alloc((void**)&d_terms, th.size() * sizeof(double)) &&
-        alloc((void**)&d_part, (size_t)nblocks * 2 * nv * sizeof(double)) &&
+        alloc((void**)&d_part, (size_t)EXPC_SECTIONS * nblocks * 2 * nv * sizeof(double)) &&
         alloc((void**)&d_out, 2 * nv * sizeof(double)) &&
         alloc((void**)&d_gpart, (size_t)gblocks * ngrid * sizeof(double)) &&
         alloc((void**)&d_gout, (size_t)ngrid * sizeof(double)) &&

@@ -11,6 +11,8 @@
 !   BasisEnlI trial loop (Kstep = 1)   -> GPU_EvalTrials(nfru,NTrials,ParSets,Energies,ErrorCodes)
 !   EnergyGA / EnergyGAM               -> GPU_EnergyGA(Nmin,Nmax,AreMatElemNeeded,WantVector,ErrorCode)
 !   EnergyGB                           -> GPU_EnergyGB(Evalue,Gradient,AreMatElemNeeded,ErrorCode)
+!   ExpectationValuesG main loop       -> GPU_ExpcVals(SymmAdaptMethod,Evalue,NumCFGridPoints,CFGrid,
+!   (src/workproc.f90:8159-8366)           NumDensGridPoints,DensGrid,MEkl_s,MEkl_e,CF,Dens)
 !
 !The Glob_* matrices live on the GPU inside the context; GPU_GetMatrices
 !copies Glob_H/Glob_S/Glob_diagS/Glob_invD back where host code (pruning,
@@ -110,6 +112,17 @@ interface
     integer(c_int), value :: nfru, nfa, needed, which
     real(c_double), intent(out) :: energy
     real(c_double), intent(out) :: grad(*)
+  end function
+  integer(c_int) function ecg_expectation_values(ctx, nbasis, masses, method, ny, ymats, ycoeffs, energy, c, &
+      ncf, cfgrid, ndens, densgrid, vals, errs, cf, dens) bind(C, name='ecg_expectation_values')
+    import :: c_int, c_double, c_ptr, c_double_complex
+    type(c_ptr), value :: ctx
+    integer(c_int), value :: nbasis, method, ny, ncf, ndens
+    real(c_double), intent(in) :: masses(*), cfgrid(*), densgrid(*)
+    integer(c_int), intent(in) :: ymats(*), ycoeffs(*)
+    real(c_double), value :: energy
+    complex(c_double_complex), intent(in) :: c(*)
+    real(c_double), intent(out) :: vals(*), errs(*), cf(*), dens(*)
   end function
   integer(c_int) function ecg_get_matrices(ctx, n, H, S, ld, diagS, diagH, invD) bind(C, name='ecg_get_matrices')
     import :: c_int, c_double, c_ptr, c_double_complex
@@ -253,6 +266,23 @@ subroutine GPU_EnergyGB(Evalue, Gradient, AreMatElemNeeded, ErrorCode)
                                     Glob_WhichEigenvalue, Evalue, Gradient)
   Glob_EnergyGBCounter = Glob_EnergyGBCounter + 1
 end subroutine GPU_EnergyGB
+
+!The accumulation loop of ExpectationValuesG, src/workproc.f90:8159-8366,
+!for functions 1..Glob_CurrBasisSize with the eigenvector Glob_c and
+!Glob_CurrEnergy = Evalue: MEkl_s / MEkl_e (NumOfExpcVals = 6 np + 9 values,
+!MEkl_e already times epsilon) and the CF / Dens sums, as the reference has
+!them after its MPI_ALLREDUCE.  Glob_diagS must be current on the device
+!(GPU_ComputeMatElem(1, Glob_CurrBasisSize) or GPU_EnergyGA).
+subroutine GPU_ExpcVals(SymmAdaptMethod, Evalue, NumCFGridPoints, CFGrid, NumDensGridPoints, DensGrid, &
+                        MEkl_s, MEkl_e, CF, Dens, ErrorCode)
+  integer, intent(in) :: SymmAdaptMethod, NumCFGridPoints, NumDensGridPoints
+  real(dprec), intent(in) :: Evalue, CFGrid(*), DensGrid(*)
+  real(dprec), intent(out) :: MEkl_s(*), MEkl_e(*), CF(*), Dens(*)
+  integer, intent(out) :: ErrorCode
+  ErrorCode = ecg_expectation_values(ecg_ctx, Glob_CurrBasisSize, Glob_Mass, SymmAdaptMethod, Glob_NumYTerms, &
+                                     Glob_YMatr, Glob_YCoeff, Evalue, Glob_c, NumCFGridPoints, CFGrid, &
+                                     NumDensGridPoints, DensGrid, MEkl_s, MEkl_e, CF, Dens)
+end subroutine GPU_ExpcVals
 
 !Copy the device matrices and vectors back into the Glob_* host arrays for
 !code that still reads them on the host.

@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--cpu-baseline", type=int, default=1)
     ap.add_argument("--candidates", type=int, default=1, help="also time the batched-candidate configuration")
     ap.add_argument("--cand-K", type=int, default=2000)
+    ap.add_argument("--expc", type=int, default=1, help="also time the expectation-value pass")
+    ap.add_argument("--expc-K", type=int, default=4000)
+    ap.add_argument("--only-expc", type=int, default=0, help="time only the expectation-value pass (profiling)")
     ap.add_argument("--lam", type=float, default=None,
                     help="use this lambda~ instead of searching for one (profiling runs)")
     return ap.parse_args()
@@ -339,6 +342,8 @@ def run_ours(args, dist):
     ctx.close()
     if args.candidates:
         line["candidates"] = run_candidates(args, dev, dist.rank, cpu=bool(args.cpu_baseline and dist.rank == 0))
+    if args.expc:
+        line["expectation_values"] = run_expc(args, dev, dist.rank, cpu=bool(args.cpu_baseline and dist.rank == 0))
     return line
 
 
@@ -478,6 +483,63 @@ def cpu_candidates(sysm, params, cands, K0, Kp=600, ntrial=8):
             "sample": f"oracle trial loop, {ntrial} candidates on a base of K'={Kp}, scaled by (K/K')^2"}
 
 
+def run_expc(args, dev, rank, cpu=True):
+    """The expectation-value pass of ExpectationValuesG (SymmAdaptMethod 1:
+    MatrixElementsForExpcVals for every pair and Y^+Y term, weighted by the
+    eigenvector) at n = 3, T = 4 on the first K functions of the seed-1002
+    basis, with the eigenvector of the 'G' solve.  Timed through the C ABI
+    with the eigenvector in host memory (copied in every call) and the
+    6np+9 sums and bounds copied back."""
+    from ecg_b200 import Context, synth
+    K = args.expc_K
+    sysm, params = synth.config_basis(CONFIG_INDEX, K=K)
+    if rank:
+        params = synth.random_basis(sysm.n, K, synth.CONFIGS[CONFIG_INDEX]["seed"] + 7919 * rank)
+    with Context(sysm, K, method="G", device=dev) as ctx:
+        ctx.set_params(params)
+        E, err, _ = ctx.energy_ga(1, K, which=1, want_vector=True)
+        c, _ = ctx.vectors(K)
+        for _ in range(max(1, min(args.warmup, 2))):
+            ctx.expectation_values(K, E, c)
+        reps = max(1, min(args.steps, 3))
+        ms = 0.0
+        l0 = ctx.launch_count()
+        for _ in range(reps):
+            ctx.timer_start()
+            d = ctx.expectation_values(K, E, c)
+            ms += ctx.timer_stop()
+        launches = (ctx.launch_count() - l0) // reps
+        ms /= reps
+    terms = K * (K + 1) // 2 * sysm.T
+    out = {"workload": f"ExpectationValuesG pass n=3 K={K} T={sysm.T} (SymmAdaptMethod 1), eigenvector of the "
+                       f"'G' solve (E = {E:.12f})",
+           "pair_terms_per_s": terms / (ms / 1e3), "ms_per_pass": ms, "gpu_launches_per_pass": int(launches),
+           "S": d["S"], "H_minus_E": d["H"] - E, "rel_err_bound_H": abs(d["H_e"] / d["H"])}
+    if cpu:
+        out["cpu_baseline"] = cpu_expc(sysm, params, terms)
+    return out
+
+
+def cpu_expc(sysm, params, terms, Kp=300):
+    """The oracle's expectation-value loop (all host threads) over the first
+    K' functions, scaled to the full pair count."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    o = orc.Oracle(sysm, Kp)
+    o.set_params(params[:Kp])
+    o.compute_mat_elem(1, Kp, 0.0, method="G")
+    c = np.ones(Kp, dtype=np.complex128)
+    t0 = time.perf_counter()
+    o.expectation_values(Kp, c, -1.0)
+    t = time.perf_counter() - t0
+    sample = Kp * (Kp + 1) // 2 * sysm.T
+    return {"value": sample / t, "unit": "pair terms/s", "cores": threads, "kind": "port",
+            "sample": f"oracle ExpectationValuesG loop over K'={Kp} functions ({sample} pair terms)",
+            "ms_per_pass_scaled": t * terms / sample * 1e3}
+
+
 def run_reference(args, dist):
     if dist.rank != 0:
         return None
@@ -509,7 +571,12 @@ def main():
     args = parse()
     dist = Dist()
     try:
-        line = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
+        if args.only_expc and args.impl == "ours":
+            import torch
+            torch.cuda.set_device(dist.local)
+            line = {"expectation_values": run_expc(args, dist.local, dist.rank, cpu=bool(args.cpu_baseline))}
+        else:
+            line = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
         if dist.rank == 0 and line is not None:
             print(json.dumps(line))
     finally:
