@@ -698,6 +698,33 @@ int ecg_energy_gb_adjoint(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, 
     return ECG_OK;
 }
 
+int ecg_overlap_penalty(ecg_ctx* ctx, int nfru, int nfa, double max_pair_overlap_penalty, double overlap_threshold2,
+                        int mode, double* total_penalty, double* grad_host)
+{
+    if (!ctx || !total_penalty) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (nfru < 0 || nfa <= nfru || nfa > c.ld || mode < 0 || mode > 2) return ECG_EARG;
+    if (cudaSetDevice(c.dev) != cudaSuccess) return ECG_ECUDA;
+    const double pc = max_pair_overlap_penalty / (1.0 - overlap_threshold2);
+    const int nfo = nfa - nfru;
+    // one partial sum per function; the solver's per-column scratch (2 ld doubles) holds them
+    double* part = c.colval;
+    CKR(launch_penalty(c, nfru, nfa, overlap_threshold2, pc, mode, part));
+    std::vector<double> h((size_t)nfo);
+    CK(cudaMemcpyAsync(h.data(), part, (size_t)nfo * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    if (mode > 0 && grad_host) {
+        CK(cudaMemcpyAsync(grad_host, c.grad, (size_t)nfo * c.npt * sizeof(double), cudaMemcpyDeviceToHost,
+                           c.stream));
+        c.bytes_d2h += (long long)nfo * c.npt * sizeof(double);
+    }
+    CK(cudaStreamSynchronize(c.stream));
+    c.bytes_d2h += (long long)nfo * sizeof(double);
+    double tp = 0.0;
+    for (int r = 0; r < nfo; r++) tp += h[r];
+    *total_penalty = tp;
+    return ECG_OK;
+}
+
 int ecg_expectation_values(ecg_ctx* ctx, int nbasis, const double* masses_host, int symm_adapt_method, int ny,
                            const int* y_mats_host, const int* y_coeffs_host, double energy, const double* c_host,
                            int ncf, const double* cf_grid_host, int ndens, const double* dens_grid_host,

@@ -196,6 +196,9 @@ int launch_term_batch(Ctx& c, int count, const double* pk, const double* pl, con
                       cd* hs, cd* dk, cd* dl);
 
 int launch_cand_rows(Ctx& c, CandWork& cw, int nbase, int count, double approx_e, int variant);
+// overlap penalty: part receives one partial sum per function nfru..nfa-1;
+// mode 0 value only, 1 adds the reference's gradient to c.grad, 2 the exact one
+int launch_penalty(Ctx& c, int nfru, int nfa, double t2, double pc, int mode, double* part);
 
 // ---- batched candidates (cand.cu) ----
 int eval_candidates(Ctx& c, int nbase, int count, const double* cand_host, double approx_e, double tol,

@@ -729,6 +729,137 @@ __global__ void __launch_bounds__(W * 32) k_cand_row(SysParams sp, const double*
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Overlap penalty, ComputeOverlapPenalty / ComputeOverlapPenaltyAndAddGradient
+// (src/workproc.f90:1491-1693): P = sum over pairs i < j, j > nfru, of
+// pc (|S~_ji|^2 - t2) where |S~_ji|^2 > t2, pc = b / (1 - t2).  One CTA per
+// function r of the optimised range; its threads scan the partners p of r in
+// the normalised overlap Glob_S (lower triangle).  The pair (j = max, i =
+// min) adds to the penalty in the CTA of its larger index.  With a gradient
+// mode, the derivatives the reference reads from Glob_D are recomputed here
+// for the flagged pairs only (usually few): the S part of Glob_D(., r-nfru,
+// p) (the pair's term sum times 1/sqrt(diagS_r diagS_p), conjugated when r
+// is the column function) and of the diagonal Glob_D(., r-nfru, r) (2 Re of
+// the term sum over diagS_r), so no derivative array is needed.  Mode 1 adds
+// the reference's expression, mode 2 the derivative of the penalty (no
+// sqrt(diagS_i/diagS_j) factor, |S~|^2 for the lower-index function).  Each
+// CTA sums its partners in a fixed order.
+// ---------------------------------------------------------------------------
+constexpr int PEN_NT = 128;
+
+template <int N>
+__device__ void pen_pair_deriv(const SysParams& sp, const double* __restrict__ coef,
+                               const double* __restrict__ Pd, const double* __restrict__ params,
+                               const cd* __restrict__ bra, const cd* __restrict__ ket,
+                               const double* __restrict__ detL, int k, int l, bool want_row, cd* out)
+{
+    // sum over terms of dS(k,l) w.r.t. the row function k (want_row) or the
+    // column function l; out receives 2 NP complex values (vech L, vech B)
+    constexpr int NP = Sym<N>::NP;
+    cd Ck[N][N];
+    load_sym<N>(bra + (size_t)k * NP, Ck);
+    double Lk[N][N], Ll[N][N];
+    load_L<N>(params + (size_t)k * 2 * NP, Lk);
+    load_L<N>(params + (size_t)l * 2 * NP, Ll);
+    const double absdet = fabs(detL[l] * detL[k]);
+    for (int m = 0; m < 2 * NP; m++) out[m] = mk(0.0, 0.0);
+    for (int t = 0; t < sp.T; t++) {
+        cd tCl[N][N];
+        load_sym<N>(ket + ((size_t)l * sp.T + t) * NP, tCl);
+        TermEnergy<N> te;
+        term_energy<N, true>(Ck, tCl, absdet, sp, te);
+        double P[N][N];
+        load_P<N>(Pd, t, P);
+        cd Dk[4 * NP], Dl[4 * NP];
+        term_grad_plain<N, true, true>(Lk, Ll, P, Ck, tCl, te, sp, Dk, Dl);
+        const double cf = coef[t];
+        const cd* d = want_row ? Dk : Dl;
+#pragma unroll
+        for (int m = 0; m < 2 * NP; m++) out[m] = rfma(cf, d[2 * NP + m], out[m]);
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(PEN_NT) k_penalty(SysParams sp, const double* __restrict__ coef,
+                                                    const double* __restrict__ Pd,
+                                                    const double* __restrict__ params, const cd* __restrict__ bra,
+                                                    const cd* __restrict__ ket, const double* __restrict__ detL,
+                                                    const double* __restrict__ diagS, const cd* __restrict__ S,
+                                                    int ld, int nfru, int nfa, double t2, double pc, int mode,
+                                                    double* __restrict__ grad, double* __restrict__ part)
+{
+    constexpr int NP = Sym<N>::NP, NPT = 2 * NP;
+    __shared__ double sg[NPT][PEN_NT];
+    __shared__ double stp[PEN_NT];
+    __shared__ double sdd[NPT];
+    const int tid = threadIdx.x;
+    const int r = nfru + blockIdx.x;
+    const double dr = diagS[r];
+    double tp = 0.0;
+    bool flagged = false;
+    for (int p = tid; p < nfa; p += PEN_NT) {
+        if (p == r) continue;
+        const int j = max(p, r), i = min(p, r);
+        const cd s = S[(size_t)j + (size_t)i * ld];
+        const double aux = s.x * s.x + s.y * s.y;
+        if (aux > t2) {
+            flagged = true;
+            if (p < r) tp += pc * (aux - t2);
+        }
+    }
+    stp[tid] = tp;
+    const int any = __syncthreads_or(flagged ? 1 : 0);
+    if (tid == 0) {
+        double a = 0.0;
+        for (int t = 0; t < PEN_NT; t++) a += stp[t];
+        part[blockIdx.x] = a;
+    }
+    if (mode == 0 || !any) return;
+    if (tid == 0) {
+        // Glob_D(npt+m, r-nfru, r) = 2 Re(sum_t coef_t dS_rr/dp_m) / diagS_r
+        cd d[NPT];
+        pen_pair_deriv<N>(sp, coef, Pd, params, bra, ket, detL, r, r, true, d);
+        for (int m = 0; m < NPT; m++) sdd[m] = 2.0 * d[m].x / dr;
+    }
+    for (int m = 0; m < NPT; m++) sg[m][tid] = 0.0;
+    __syncthreads();
+    const double temp1 = 2.0 * pc;
+    for (int p = tid; p < nfa; p += PEN_NT) {
+        if (p == r) continue;
+        const int j = max(p, r), i = min(p, r);
+        const cd s = S[(size_t)j + (size_t)i * ld];
+        const double aux = s.x * s.x + s.y * s.y;
+        if (!(aux > t2)) continue;
+        cd d[NPT];
+        const bool row = (r == j);
+        pen_pair_deriv<N>(sp, coef, Pd, params, bra, ket, detL, j, i, row, d);
+        const double f = 1.0 / sqrt(diagS[j] * diagS[i]);
+        const double temp2 = (mode == 2) ? 1.0 : sqrt(diagS[i] / diagS[j]);
+        for (int m = 0; m < NPT; m++) {
+            cd g;
+            if (row) {
+                // Glob_D(npt+m, j-nfru, i) = f dS_ji/dp_j
+                const cd dji = f * d[m];
+                const cd x = dji - (0.5 * sdd[m] * temp2) * s;
+                g = s * conj(x);
+            } else {
+                // Glob_D(npt+m, i-nfru, j) = conj(f dS_ji/dp_i)
+                const cd dij = conj(f * d[m]);
+                const cd sn = (mode == 2) ? conj(s) : s;
+                const cd x = dij - (0.5 * sdd[m] / temp2) * sn;
+                g = s * x;
+            }
+            sg[m][tid] += temp1 * g.x;
+        }
+    }
+    __syncthreads();
+    for (int m = tid; m < NPT; m += PEN_NT) {
+        double a = 0.0;
+        for (int t = 0; t < PEN_NT; t++) a += sg[m][t];
+        grad[(size_t)(r - nfru) * NPT + m] += a;
+    }
+}
+
 #define ECG_DISPATCH_N(n, FN, ...)              \
     switch (n) {                                \
         case 2: return FN<2>(__VA_ARGS__);      \
@@ -766,6 +897,19 @@ static int diag_n(Ctx& c, int r0, int r1, double approx_e, int deriv, int nfru)
     c.launches++;
     return last_err();
 }
+template <int N>
+static int penalty_n(Ctx& c, int nfru, int nfa, double t2, double pc, int mode, double* part)
+{
+    k_penalty<N><<<nfa - nfru, PEN_NT, 0, c.stream>>>(c.sp, c.coef, c.Pd, c.params, c.bra, c.ket, c.detL, c.diagS,
+                                                      c.S, c.ld, nfru, nfa, t2, pc, mode, c.grad, part);
+    c.launches++;
+    return last_err();
+}
+int launch_penalty(Ctx& c, int nfru, int nfa, double t2, double pc, int mode, double* part)
+{
+    ECG_DISPATCH_N(c.n, penalty_n, c, nfru, nfa, t2, pc, mode, part)
+}
+
 int launch_pair_diag(Ctx& c, int r0, int r1, double approx_e, int deriv, int nfru)
 {
     ECG_DISPATCH_N(c.n, diag_n, c, r0, r1, approx_e, deriv, nfru)

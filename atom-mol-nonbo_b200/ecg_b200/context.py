@@ -202,6 +202,19 @@ class Context:
                                                     int(which), C.byref(e), dptr(g)), "ecg_energy_gb_adjoint")
         return e.value, g, err
 
+    def overlap_penalty(self, nfru, nfa, max_pair_overlap_penalty, overlap_threshold2, mode=0):
+        """ComputeOverlapPenalty (mode 0) / ComputeOverlapPenaltyAndAddGradient
+        (mode 1: the reference's gradient added to the context's gradient;
+        mode 2: the exact derivative of the penalty instead),
+        src/workproc.f90:1491-1693.  Returns (TotalPenalty, updated gradient
+        or None)."""
+        tp = C.c_double()
+        g = np.zeros((nfa - nfru) * self.npt) if mode else None
+        _check(self.lib.ecg_overlap_penalty(self.h, int(nfru), int(nfa), float(max_pair_overlap_penalty),
+                                            float(overlap_threshold2), int(mode), C.byref(tp), dptr(g)),
+               "ecg_overlap_penalty")
+        return tp.value, g
+
     def expectation_values(self, nbasis, energy, c=None, method=1, cf_grid=None, dens_grid=None, raw=False):
         """The expectation-value pass of ExpectationValuesG
         (src/workproc.f90:8159-8366) over functions 1..nbasis with the

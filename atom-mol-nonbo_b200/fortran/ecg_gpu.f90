@@ -11,6 +11,7 @@
 !   BasisEnlI trial loop (Kstep = 1)   -> GPU_EvalTrials(nfru,NTrials,ParSets,Energies,ErrorCodes)
 !   EnergyGA / EnergyGAM               -> GPU_EnergyGA(Nmin,Nmax,AreMatElemNeeded,WantVector,ErrorCode)
 !   EnergyGB                           -> GPU_EnergyGB(Evalue,Gradient,AreMatElemNeeded,ErrorCode)
+!   ComputeOverlapPenalty(AndAddGradient) -> GPU_OverlapPenalty(AddGradient,TotalPenalty,Gradient)
 !   ExpectationValuesG main loop       -> GPU_ExpcVals(SymmAdaptMethod,Evalue,NumCFGridPoints,CFGrid,
 !   (src/workproc.f90:8159-8366)           NumDensGridPoints,DensGrid,MEkl_s,MEkl_e,CF,Dens)
 !
@@ -112,6 +113,15 @@ interface
     integer(c_int), value :: nfru, nfa, needed, which
     real(c_double), intent(out) :: energy
     real(c_double), intent(out) :: grad(*)
+  end function
+  integer(c_int) function ecg_overlap_penalty(ctx, nfru, nfa, maxpen, thr2, mode, total, grad) &
+      bind(C, name='ecg_overlap_penalty')
+    import :: c_int, c_double, c_ptr
+    type(c_ptr), value :: ctx
+    integer(c_int), value :: nfru, nfa, mode
+    real(c_double), value :: maxpen, thr2
+    real(c_double), intent(out) :: total
+    real(c_double), intent(inout) :: grad(*)
   end function
   integer(c_int) function ecg_expectation_values(ctx, nbasis, masses, method, ny, ymats, ycoeffs, energy, c, &
       ncf, cfgrid, ndens, densgrid, vals, errs, cf, dens) bind(C, name='ecg_expectation_values')
@@ -266,6 +276,21 @@ subroutine GPU_EnergyGB(Evalue, Gradient, AreMatElemNeeded, ErrorCode)
                                     Glob_WhichEigenvalue, Evalue, Gradient)
   Glob_EnergyGBCounter = Glob_EnergyGBCounter + 1
 end subroutine GPU_EnergyGB
+
+!ComputeOverlapPenalty (AddGradient=.false.) and
+!ComputeOverlapPenaltyAndAddGradient (.true.), src/workproc.f90:1491-1693,
+!on the device's Glob_S: TotalPenalty, and with AddGradient the reference's
+!penalty gradient added to the gradient the last GPU_EnergyIB/GB left on the
+!device, returned in Gradient (npt * nfo).  Called where EnergyGA/GB call
+!the reference routines (src/workproc.f90:1759,1824,1943).
+subroutine GPU_OverlapPenalty(AddGradient, TotalPenalty, Gradient)
+  logical, intent(in) :: AddGradient
+  real(dprec), intent(out) :: TotalPenalty
+  real(dprec), intent(inout) :: Gradient(*)
+  integer(c_int) :: st
+  st = ecg_overlap_penalty(ecg_ctx, Glob_nfru, Glob_nfa, Glob_MaxOverlapPenalty, Glob_OverlapPenaltyThreshold2, &
+                           merge(1, 0, AddGradient), TotalPenalty, Gradient)
+end subroutine GPU_OverlapPenalty
 
 !The accumulation loop of ExpectationValuesG, src/workproc.f90:8159-8366,
 !for functions 1..Glob_CurrBasisSize with the eigenvector Glob_c and

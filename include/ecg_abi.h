@@ -145,6 +145,24 @@ int ecg_energy_ga(ecg_ctx* ctx, int nmin, int nmax, int mat_elem_needed, int whi
 int ecg_energy_gb_adjoint(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, int which, double* energy,
                           double* grad_host);
 
+/* ComputeOverlapPenalty (mode 0) and ComputeOverlapPenaltyAndAddGradient
+ * (mode 1), src/workproc.f90:1491-1693: total_penalty = sum over pairs
+ * i < j <= nfa with j > nfru of b (|S_ji|^2 - t2) / (1 - t2) where
+ * |S_ji|^2 > t2, from the normalised overlaps in Glob_S (b =
+ * max_pair_overlap_penalty = Glob_MaxOverlapPenalty, t2 =
+ * overlap_threshold2 = Glob_OverlapPenaltyThreshold2).  Mode 1 adds the
+ * reference's penalty gradient to the context's gradient (the one the last
+ * ecg_energy_ib* / ecg_energy_gb_adjoint call left, Glob_WkGR), with the
+ * derivatives it reads from Glob_D recomputed for the flagged pairs, so the
+ * fused adjoint path needs no Glob_D.  Mode 2 adds instead the derivative
+ * of the penalty itself: the reference's normalisation terms carry a factor
+ * sqrt(diagS_i/diagS_j), and for the lower-index function S_ji^2 where the
+ * derivative has |S_ji|^2.  grad_host (may be NULL) receives the updated gradient (npt x
+ * (nfa - nfru)).  Requires Glob_S, Glob_diagS and the parameters of
+ * functions 1..nfa current (any ComputeMatElem over them). */
+int ecg_overlap_penalty(ecg_ctx* ctx, int nfru, int nfa, double max_pair_overlap_penalty, double overlap_threshold2,
+                        int mode, double* total_penalty, double* grad_host);
+
 /* The expectation-value pass of ExpectationValuesG, src/workproc.f90:
  * 8159-8366, with MatrixElementsForExpcVals (src/matelem.f90:949-1983) for
  * every pair of functions 1..nbasis and every symmetry term:

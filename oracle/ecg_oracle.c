@@ -22,6 +22,8 @@
  *                                            1598-1629,1413-1443
  *   GHEPIIS                   src/linalg.f90:1781-1926
  *   EnergyIA/IAM/IB glue      src/workproc.f90:1954-2154
+ *   ComputeOverlapPenalty(AndAddGradient)
+ *                             src/workproc.f90:1491-1693
  *
  * The MPI work split of the reference is replaced by an OpenMP loop over
  * pairs; every pair element is computed exactly as one MPI rank computes it
@@ -858,6 +860,67 @@ void orc_gradient_contract(int nfo, int nfa, int nfru, const cplx *D, int ldo, c
                       t * conj(t) * (D[DX(m, k, k + nfru)] - E * D[DX(m + npt, k, k + nfru)]));
     }
 #undef DX
+}
+
+/* ComputeOverlapPenalty (WkGR == NULL) and ComputeOverlapPenaltyAndAddGradient
+ * (WkGR != NULL: the penalty gradient is added to it), src/workproc.f90:
+ * 1491-1693, NumOfProcs = 1 branch.  S is Glob_S (its strict lower triangle
+ * is read, S(j,i) with j > i), D is Glob_D as orc_gradient_contract takes it.
+ * Returns TotalPenalty.
+ * exact = 1 replaces the reference's gradient by the derivative of its
+ * penalty: the reference's normalisation terms carry a factor
+ * sqrt(diagS_i/diagS_j) and, for the function of the lower index, S_ji^2
+ * where the derivative has |S_ji|^2 and conj(Glob_D(.,i-nfru,j)). */
+double orc_overlap_penalty(int nfru, int nfa, double max_pen, double thr2, const cplx *S, int ld,
+                           const double *diagS, const cplx *D, int ldo, double *WkGR, int exact)
+{
+    const int npt = g_npt, n2 = 2 * g_npt;
+#define DX(m, a, b) ((size_t)(m) + (size_t)((a) - 1) * n2 + (size_t)((b) - 1) * (size_t)n2 * ldo)
+#define SX(j, i) ((size_t)((j) - 1) + (size_t)((i) - 1) * (size_t)ld)
+    double tp = 0.0, aux, temp2;
+    const double pen_coeff = max_pen / (1.0 - thr2);
+    const double temp1 = 2 * pen_coeff;
+    for (int i = 1; i <= nfru; i++)
+        for (int j = nfru + 1; j <= nfa; j++) {
+            const cplx Sji = S[SX(j, i)];
+            aux = creal(Sji) * creal(Sji) + cimag(Sji) * cimag(Sji);
+            if (aux > thr2) {
+                tp = tp + pen_coeff * (aux - thr2);
+                if (WkGR) {
+                    temp2 = exact ? 1.0 : sqrt(diagS[i - 1] / diagS[j - 1]);
+                    for (int m = 1; m <= npt; m++)
+                        WkGR[(size_t)(j - nfru - 1) * npt + m - 1] =
+                            WkGR[(size_t)(j - nfru - 1) * npt + m - 1] +
+                            temp1 * creal(Sji * conj(D[DX(npt + m - 1, j - nfru, i)] -
+                                                     0.5 * D[DX(npt + m - 1, j - nfru, j)] * Sji * temp2));
+                }
+            }
+        }
+    for (int i = nfru + 1; i <= nfa; i++)
+        for (int j = i + 1; j <= nfa; j++) {
+            const cplx Sji = S[SX(j, i)];
+            aux = creal(Sji) * creal(Sji) + cimag(Sji) * cimag(Sji);
+            if (aux > thr2) {
+                tp = tp + pen_coeff * (aux - thr2);
+                if (WkGR) {
+                    temp2 = exact ? 1.0 : sqrt(diagS[i - 1] / diagS[j - 1]);
+                    const cplx Sn = exact ? conj(Sji) : Sji;
+                    for (int m = 1; m <= npt; m++)
+                        WkGR[(size_t)(i - nfru - 1) * npt + m - 1] =
+                            WkGR[(size_t)(i - nfru - 1) * npt + m - 1] +
+                            temp1 * creal(Sji * (D[DX(npt + m - 1, i - nfru, j)] -
+                                                 0.5 * D[DX(npt + m - 1, i - nfru, i)] * Sn / temp2));
+                    for (int m = 1; m <= npt; m++)
+                        WkGR[(size_t)(j - nfru - 1) * npt + m - 1] =
+                            WkGR[(size_t)(j - nfru - 1) * npt + m - 1] +
+                            temp1 * creal(Sji * conj(D[DX(npt + m - 1, j - nfru, i)] -
+                                                     0.5 * D[DX(npt + m - 1, j - nfru, j)] * Sji * temp2));
+                }
+            }
+        }
+#undef DX
+#undef SX
+    return tp;
 }
 
 void orc_set_threads(int nt)

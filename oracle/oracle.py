@@ -57,6 +57,9 @@ def load():
                                                C.c_double, C.c_int, _dp, C.c_int, _dp, _dp, _dp, _dp, _dp]
         lib.orc_set_masses_ld.argtypes = [_dp]
         lib.orc_expectation_values_ld.argtypes = lib.orc_expectation_values.argtypes
+        lib.orc_overlap_penalty.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _dp, C.c_int, _dp, _dp,
+                                            C.c_int, _dp, C.c_int]
+        lib.orc_overlap_penalty.restype = C.c_double
         lib.orc_set_threads.argtypes = [C.c_int]
         lib.orc_get_threads.restype = C.c_int
         _lib = lib
@@ -165,6 +168,21 @@ class Oracle:
         g = np.zeros(nfo * self.npt)
         self.lib.orc_gradient_contract(nfo, nfa, nfru, _p(self.D), self.D.shape[1], _p(self.c), E, _p(g))
         return E, g, err, it
+
+    # ComputeOverlapPenalty(AndAddGradient), src/workproc.f90:1491-1693
+    def overlap_penalty(self, nfru, nfa, max_pen, thr2, WkGR=None, exact=False):
+        """TotalPenalty from this oracle's Glob_S; with WkGR (npt * nfo
+        array) the penalty gradient is added to it in place (needs Glob_D,
+        as left by compute_mat_elem_and_deriv): the reference's formula, or
+        with exact=True the derivative of the penalty."""
+        wk = None
+        if WkGR is not None:
+            assert WkGR.dtype == np.float64 and WkGR.flags.c_contiguous
+            wk = _p(WkGR)
+        D = self.D if self.D is not None else np.zeros(1, dtype=np.complex128)
+        ldo = self.D.shape[1] if self.D is not None else 1
+        return self.lib.orc_overlap_penalty(nfru, nfa, max_pen, thr2, _p(self.S), self.ld, _p(self.diagS), _p(D),
+                                            ldo, wk, int(exact))
 
     # ExpectationValuesG term lists, src/workproc.f90:8175-8347
     def expc_terms(self, method):
