@@ -68,13 +68,22 @@ __global__ void __launch_bounds__(256) k_ldl_mirror(cd* __restrict__ A, int ld, 
 //   (b) one thread per column c beyond the sub-block forms the unscaled
 //       rows Wun(q, c) = W(q, c) - sum_{q' < q} conj(U(q', q)) Wun(q', c)
 //       by substitution and U(q, c) = invD_q Wun(q, c);
-//   (c) all threads apply the rank-8 update W(r, c) -= sum_q conj(U(q, r))
-//       Wun(q, c) to the rows and columns beyond the sub-panel.
+//   (c) the eight warps apply the rank-8 update W(r, c) -= sum_q
+//       conj(U(q, r)) Wun(q, c) to the rows and columns beyond the
+//       sub-panel on the FP64 tensor cores.
 // Three barriers per sub-panel.  The recurrence and the pivot
 // d = conj(W(q, q)) follow src/linalg.f90:359-391; pivots are real (the
 // imaginary part of W(q, q) is rounding noise of the updates and is
 // dropped: kept, it sets a floor of 1e-13..1e-12 under GHEPIIS's residual
 // NormOfDiff).
+// one m8n8k4 FP64 tensor-core product, D = A B + C (C = D in place)
+__device__ __forceinline__ void mma_f64(double& c0, double& c1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
 constexpr int DG_LD = LDL_NB + 1;
 constexpr int DG_SUB = 8;
 constexpr size_t DG_SMEM = (size_t)(LDL_NB * DG_LD + DG_SUB * LDL_NB) * sizeof(double2);
@@ -168,48 +177,53 @@ __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, in
             }
         }
         __syncthreads();
-        // (c) rank-8 update of the rows and columns beyond the sub-panel:
-        // thread (rr, cc) owns rows t0 + rr + 16 i and columns t0 + cc + 16 j
+        // (c) rank-8 update of the rows and columns beyond the sub-panel on
+        // the FP64 tensor cores: 8 x 8 output tiles of the upper triangle
+        // (tile row <= tile column) spread over the eight warps; per tile
+        // and k-step of 4, four m8n8k4 products with the conjugate and the
+        // minus sign folded into the U fragment, accumulated onto W.
         if (t0 < b) {
-            const int rr = tid >> 4, cc = tid & 15;
-            const int nblk = (b - t0 + 15) >> 4;  // 16-wide blocks of the trailing part
-            cd acc[4][4];
+            const int lane = tid & 31, wp = tid >> 5;
+            const int g = lane >> 2, t4 = lane & 3;
+            const int T = (b - t0 + 7) >> 3;
+            const int ntiles = T * (T + 1) / 2;
+            for (int tile = wp; tile < ntiles; tile += 8) {
+                int R = 0, rem = tile;
+                while (rem >= T - R) {
+                    rem -= T - R;
+                    R++;
+                }
+                const int Cc = R + rem;
+                const int r = t0 + 8 * R + g;         // fragment row (C and U)
+                const int cg = t0 + 8 * Cc + g;       // fragment column of Wun
+                const int ca = t0 + 8 * Cc + 2 * t4;  // C columns ca, ca + 1
+                double accr[2], acci[2];
 #pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int jj = 0; jj < 4; jj++) {
-                    const int r = t0 + rr + 16 * i, c = t0 + cc + 16 * jj;
+                for (int e = 0; e < 2; e++) {
+                    const int c = ca + e;
                     double2 w = make_double2(0.0, 0.0);
                     if (r < b && c < b && r <= c) w = Ws[r * DG_LD + c];
-                    acc[i][jj] = cd{w.x, w.y};
+                    accr[e] = w.x;
+                    acci[e] = w.y;
                 }
 #pragma unroll
-            for (int q = 0; q < DG_SUB; q++) {
-                if (q < nq) {
-                    cd u[4], v[4];
+                for (int k0 = 0; k0 < DG_SUB; k0 += 4) {
+                    const int q = k0 + t4;
+                    double2 u = make_double2(0.0, 0.0), v = make_double2(0.0, 0.0);
+                    if (q < nq && r < b) u = Ws[(s0 + q) * DG_LD + r];  // U(q, r)
+                    if (q < nq && cg < b) v = Wu[q * LDL_NB + cg];      // Wun(q, c)
+                    // W -= conj(U) Wun: Re -= Ur Vr + Ui Vi, Im -= Ur Vi - Ui Vr
+                    mma_f64(accr[0], accr[1], -u.x, v.x);
+                    mma_f64(accr[0], accr[1], -u.y, v.y);
+                    mma_f64(acci[0], acci[1], -u.x, v.y);
+                    mma_f64(acci[0], acci[1], u.y, v.x);
+                }
 #pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        const int r = t0 + rr + 16 * i;
-                        const double2 x = (r < b) ? Ws[(s0 + q) * DG_LD + r] : make_double2(0.0, 0.0);  // U(q, r)
-                        u[i] = cd{x.x, -x.y};
-                        const int c = t0 + cc + 16 * i;
-                        const double2 y = (c < b) ? Wu[q * LDL_NB + c] : make_double2(0.0, 0.0);  // Wun(q, c)
-                        v[i] = cd{y.x, y.y};
-                    }
-#pragma unroll
-                    for (int i = 0; i < 4; i++)
-#pragma unroll
-                        for (int jj = 0; jj < 4; jj++)
-                            if (i <= jj && jj < nblk) acc[i][jj] = cfms(u[i], v[jj], acc[i][jj]);  // block-uniform
+                for (int e = 0; e < 2; e++) {
+                    const int c = ca + e;
+                    if (r < b && c < b && r <= c) Ws[r * DG_LD + c] = make_double2(accr[e], acci[e]);
                 }
             }
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int jj = 0; jj < 4; jj++) {
-                    const int r = t0 + rr + 16 * i, c = t0 + cc + 16 * jj;
-                    if (r < b && c < b && r <= c) Ws[r * DG_LD + c] = make_double2(acc[i][jj].x, acc[i][jj].y);
-                }
         }
         __syncthreads();
     }
@@ -345,12 +359,6 @@ constexpr int UPD_KC = 32;
 constexpr int UPD_LD = 68;
 constexpr size_t UPD_SMEM = 4 * UPD_KC * UPD_LD * sizeof(double);
 
-__device__ __forceinline__ void mma_f64(double& c0, double& c1, double a, double b)
-{
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(c0), "+d"(c1)
-                 : "d"(a), "d"(b));
-}
 
 template <int TC, int WR, int WC>
 __global__ void __launch_bounds__(256, 2) k_ldl_update(cd* __restrict__ A, int ld, int p0, int p1, int r0, int rend,
