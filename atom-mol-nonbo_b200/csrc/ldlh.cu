@@ -12,7 +12,7 @@
 //   k_ldl_diag    eliminate the 64 x 64 diagonal block in shared memory,
 //                 producing U (= L^H) and invD;
 //   k_ldl_trsm    Wun(p, c) by substitution with U_pp, U(p, c) = invD Wun;
-//   k_ldl_update  W(r, c) -= sum_q conj(U(q,r)) Wun(q,c), r <= c beyond p
+//   k_ldl_bulk    W(r, c) -= sum_q conj(U(q,r)) Wun(q,c), r <= c beyond p
 //                 (the Hermitian rank-64 trailing update, a complex GEMM);
 //   k_ldl_linv    after the last panel: (U_pp^H)^-1 of every new panel.
 // The off-diagonal recurrence and the pivot d = conj(.) follow
@@ -20,6 +20,7 @@
 // and the pivots are kept real (the reference's complex arithmetic leaves a
 // rounding-level imaginary part in them).
 #include "ecg_internal.h"
+#include "zmma.cuh"
 
 namespace ecg {
 
@@ -346,37 +347,36 @@ __global__ void __launch_bounds__(256) k_ldl_trsm(cd* __restrict__ A, int ld, in
     }
 }
 
-// Trailing update over 64 x 64 output tiles on the FP64 tensor cores:
+// Trailing update over 64 x TC output tiles on the FP64 tensor cores:
 //   W(r, c) -= sum_q conj(U(q, r)) Wun(q, c),  r in [r0, rend), c in [max(r, c0), n)
-// with mma.sync.m8n8k4.f64.  Eight warps as 2 x 4, each a 32 x 16 complex
-// sub-tile (4 x 2 tiles of 8 x 8); per tile and k-step of 4 the real and
-// imaginary accumulators take four mma: Re += Ur Vr + Ui Vi and
+// with mma.sync.m8n8k4.f64.  Eight warps as WR x WC, each a (64/WR) x
+// (TC/WC) complex sub-tile of 8 x 8 tiles; per tile and k-step of 4 the real
+// and imaginary accumulators take four mma: Re += Ur Vr + Ui Vi and
 // Im += Ur Vi + (-Ui) Vr (the conjugate folded into a negated fragment).
-// Panel rows are staged through shared memory in chunks of 32 with real and
-// imaginary parts in separate arrays (row pitch 68 doubles: the four k rows
-// of a fragment load fall in distinct banks).
-constexpr int UPD_KC = 32;
-constexpr int UPD_LD = 68;
-constexpr size_t UPD_SMEM = 4 * UPD_KC * UPD_LD * sizeof(double);
-
+// U and Wun are staged by cp.async in two buffers of 16 k rows each, so that
+// the next chunk streams in while the current one is multiplied; complex
+// values stay interleaved in shared memory with a pitch of 66 double2
+// (= 2 mod 8 slots of 16 B), so the fragment loads of a warp are
+// conflict-free.  <64, 2, 4>: the bulk (64 x 64 tiles, side stream);
+// <16, 8, 1>: the rows of the next panel (64 x 16 tiles, enough CTAs for one
+// row of tiles, main stream).
+constexpr int BLK_KC = 16;
+constexpr int BLK_P = 66;
+constexpr size_t BLK_SMEM = 2 * 2 * BLK_KC * BLK_P * sizeof(double2);
 
 template <int TC, int WR, int WC>
-__global__ void __launch_bounds__(256, 2) k_ldl_update(cd* __restrict__ A, int ld, int p0, int p1, int r0, int rend,
-                                                     int c0, int n, const cd* __restrict__ vbuf, cd* __restrict__ dw)
+__global__ void __launch_bounds__(256, 2) k_ldl_bulk(cd* __restrict__ A, int ld, int p0, int p1, int r0, int rend,
+                                                   int c0, int n, const cd* __restrict__ vbuf, cd* __restrict__ dw)
 {
     constexpr int MT = LDL_NB / WR / 8;  // 8 x 8 tiles per warp along rows
     constexpr int NT = TC / WC / 8;      // and along columns
-    extern __shared__ double smd[];
-    double* Ur = smd;                       // [k][m]
-    double* Ui = Ur + UPD_KC * UPD_LD;
-    double* Vr = Ui + UPD_KC * UPD_LD;      // [k][n]
-    double* Vi = Vr + UPD_KC * UPD_LD;
+    extern __shared__ double2 sb[];
     const int rb = r0 + blockIdx.y * LDL_NB;
     const int cb = c0 + blockIdx.x * TC;
     if (rb > cb + TC - 1) return;  // tile entirely below the diagonal
     const int b = p1 - p0;
     const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-    const int wr = wp / WC, wc = wp % WC;  // warp rows MT*8*wr, columns NT*8*wc
+    const int wr = wp / WC, wc = wp % WC;
     const int g = lane >> 2, t4 = lane & 3;
     double accr[MT][NT][2], acci[MT][NT][2];
 #pragma unroll
@@ -385,8 +385,29 @@ __global__ void __launch_bounds__(256, 2) k_ldl_update(cd* __restrict__ A, int l
         for (int nt = 0; nt < NT; nt++)
 #pragma unroll
             for (int e = 0; e < 2; e++) accr[mt][nt][e] = acci[mt][nt][e] = 0.0;
-    // the tile's current values, loaded together up front so that their
-    // latency overlaps the products (stored back after them)
+    auto stage = [&](int ch, int buf) {
+        const int k0 = ch * BLK_KC;
+        double2* Us = sb + buf * 2 * BLK_KC * BLK_P;
+        double2* Vs = Us + BLK_KC * BLK_P;
+        for (int e = tid; e < BLK_KC * LDL_NB; e += 256) {
+            const int q = e % BLK_KC, mm = e / BLK_KC;
+            const int r = rb + mm;
+            const bool ku = (k0 + q < b) && (r < rend);
+            cp_async16(Us + q * BLK_P + mm, ku ? (const void*)(A + (size_t)(p0 + k0 + q) + (size_t)r * ld) : (const void*)A,
+                       ku ? 16 : 0);
+        }
+        for (int e = tid; e < BLK_KC * TC; e += 256) {
+            const int q = e % BLK_KC, mm = e / BLK_KC;
+            const int c = cb + mm;
+            const bool kv = (k0 + q < b) && (c < n);
+            cp_async16(Vs + q * BLK_P + mm,
+                       kv ? (const void*)(vbuf + (size_t)(k0 + q) + (size_t)c * LDL_NB) : (const void*)vbuf, kv ? 16 : 0);
+        }
+        cp_async_commit();
+    };
+    const int nch = (b + BLK_KC - 1) / BLK_KC;
+    stage(0, 0);
+    // the tile's current values, loaded while the first chunk streams in
     double2 old[MT][NT][2];
 #pragma unroll
     for (int mt = 0; mt < MT; mt++)
@@ -402,48 +423,32 @@ __global__ void __launch_bounds__(256, 2) k_ldl_update(cd* __restrict__ A, int l
                                  : *reinterpret_cast<const double2*>(A + (size_t)r + (size_t)c * ld);
                 old[mt][nt][e] = v;
             }
-    for (int k0 = 0; k0 < b; k0 += UPD_KC) {
-        for (int e = tid; e < UPD_KC * LDL_NB; e += blockDim.x) {
-            const int q = e % UPD_KC, mm = e / UPD_KC;
-            const int r = rb + mm;
-            cd u = cd{0.0, 0.0};
-            if (k0 + q < b && r < rend) u = A[(size_t)(p0 + k0 + q) + (size_t)r * ld];
-            Ur[q * UPD_LD + mm] = u.x;
-            Ui[q * UPD_LD + mm] = u.y;
-        }
-        for (int e = tid; e < UPD_KC * TC; e += blockDim.x) {
-            const int q = e % UPD_KC, mm = e / UPD_KC;
-            const int c = cb + mm;
-            cd v = cd{0.0, 0.0};
-            if (k0 + q < b && c < n) v = ldg2(vbuf + (size_t)(k0 + q) + (size_t)c * LDL_NB);
-            Vr[q * UPD_LD + mm] = v.x;
-            Vi[q * UPD_LD + mm] = v.y;
+    for (int ch = 0; ch < nch; ch++) {
+        if (ch + 1 < nch) {
+            stage(ch + 1, (ch + 1) & 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
-#pragma unroll 2
-        for (int kk = 0; kk < UPD_KC; kk += 4) {
-            const int kr = (kk + t4) * UPD_LD;
-            double ar[MT], ai[MT], br[NT], bi[NT];
+        const double2* Us = sb + (ch & 1) * 2 * BLK_KC * BLK_P;
+        const double2* Vs = Us + BLK_KC * BLK_P;
 #pragma unroll
-            for (int mt = 0; mt < MT; mt++) {
-                const int m = (wr * MT + mt) * 8 + g;
-                ar[mt] = Ur[kr + m];
-                ai[mt] = Ui[kr + m];
-            }
+        for (int kk = 0; kk < BLK_KC; kk += 4) {
+            const int kr = (kk + t4) * BLK_P;
+            double2 a[MT], v[NT];
 #pragma unroll
-            for (int nt = 0; nt < NT; nt++) {
-                const int nn = (wc * NT + nt) * 8 + g;
-                br[nt] = Vr[kr + nn];
-                bi[nt] = Vi[kr + nn];
-            }
+            for (int mt = 0; mt < MT; mt++) a[mt] = Us[kr + (wr * MT + mt) * 8 + g];
+#pragma unroll
+            for (int nt = 0; nt < NT; nt++) v[nt] = Vs[kr + (wc * NT + nt) * 8 + g];
 #pragma unroll
             for (int mt = 0; mt < MT; mt++)
 #pragma unroll
                 for (int nt = 0; nt < NT; nt++) {
-                    mma_f64(accr[mt][nt][0], accr[mt][nt][1], ar[mt], br[nt]);
-                    mma_f64(accr[mt][nt][0], accr[mt][nt][1], ai[mt], bi[nt]);
-                    mma_f64(acci[mt][nt][0], acci[mt][nt][1], ar[mt], bi[nt]);
-                    mma_f64(acci[mt][nt][0], acci[mt][nt][1], -ai[mt], br[nt]);
+                    mma_f64(accr[mt][nt][0], accr[mt][nt][1], a[mt].x, v[nt].x);
+                    mma_f64(accr[mt][nt][0], accr[mt][nt][1], a[mt].y, v[nt].y);
+                    mma_f64(acci[mt][nt][0], acci[mt][nt][1], a[mt].x, v[nt].y);
+                    mma_f64(acci[mt][nt][0], acci[mt][nt][1], -a[mt].y, v[nt].x);
                 }
         }
         __syncthreads();
@@ -459,7 +464,6 @@ __global__ void __launch_bounds__(256, 2) k_ldl_update(cd* __restrict__ A, int l
                 if (r >= rend || c >= n || c < r) continue;
                 const double vr = accr[mt][nt][e], vi = acci[mt][nt][e];
                 const double2 o = old[mt][nt][e];
-                // diagonal: dw -= conj(sum conj(U) Wun) = sum conj(Wun) U (src/linalg.f90:370-372)
                 if (c == r)
                     *reinterpret_cast<double2*>(dw + c) = make_double2(o.x - vr, o.y + vi);
                 else
@@ -479,10 +483,10 @@ static void launch_update(Ctx& c, cudaStream_t st, const cd* vb, int p0, int p1,
         // one panel of rows (the lookahead rows): narrow 64 x 16 tiles so
         // that enough CTAs run
         dim3 g((n - c0 + 15) / 16, 1);
-        k_ldl_update<16, 8, 1><<<g, 256, UPD_SMEM, st>>>(c.F, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
+        k_ldl_bulk<16, 8, 1><<<g, 256, BLK_SMEM, st>>>(c.F, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
     } else {
         dim3 g((n - c0 + LDL_NB - 1) / LDL_NB, nrb);
-        k_ldl_update<64, 2, 4><<<g, 256, UPD_SMEM, st>>>(c.F, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
+        k_ldl_bulk<64, 2, 4><<<g, 256, BLK_SMEM, st>>>(c.F, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
     }
     c.launches++;
 }
@@ -562,8 +566,8 @@ int ldlh_factor(Ctx& c, int m0, int n)
         cudaFuncSetAttribute(k_ldl_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
         cudaFuncSetAttribute(k_ldl_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DG_SMEM);
         cudaFuncSetAttribute(k_ldl_linv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * sm1));
-        cudaFuncSetAttribute(k_ldl_update<64, 2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UPD_SMEM);
-        cudaFuncSetAttribute(k_ldl_update<16, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UPD_SMEM);
+        cudaFuncSetAttribute(k_ldl_bulk<64, 2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BLK_SMEM);
+        cudaFuncSetAttribute(k_ldl_bulk<16, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BLK_SMEM);
         g_ldl_attr = true;
     }
     // block list: existing blocks truncated at m0, then new 64-row blocks

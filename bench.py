@@ -304,7 +304,7 @@ def run_ours(args, dist):
         "pairs_hs": roof("fp64", hs_flop, st[0], peak_fma, "TFLOP/s",
                          "k_pair_energy<3> (+ k_pair_diag, k_prep): one launch per step", fma_src, "pairs_hs"),
         "ldlh": roof("tensor", ldl_flop, st[1], peak_tc, "TFLOP/s",
-                     "LDL^H factorisation, one CUDA-graph launch per step: k_ldl_update trailing updates on the "
+                     "LDL^H factorisation, one CUDA-graph launch per step: k_ldl_bulk trailing updates on the "
                      "FP64 tensor cores, k_ldl_diag / k_ldl_trsm panel kernels", tc_src, "ldlh"),
         "invit": roof("hbm", invit_bytes, st[2], peaks["hbm_gbs"], "GB/s",
                       "inverse iterations (k_hemv, k_fwd_coop, k_bwd_coop) + Rayleigh quotient", hbm_src, "invit"),
