@@ -357,7 +357,9 @@ __global__ void __launch_bounds__(256) k_ldl_trsm(cd* __restrict__ A, int ld, in
 // the next chunk streams in while the current one is multiplied; complex
 // values stay interleaved in shared memory with a pitch of 66 double2
 // (= 2 mod 8 slots of 16 B), so the fragment loads of a warp are
-// conflict-free.  <64, 2, 4>: the bulk (64 x 64 tiles, side stream);
+// conflict-free.  The tile's old values are read after the products (kept
+// out of registers during them, so three CTAs fit on an SM).
+// <64, 2, 4>: the bulk (64 x 64 tiles, side stream);
 // <16, 8, 1>: the rows of the next panel (64 x 16 tiles, enough CTAs for one
 // row of tiles, main stream).
 constexpr int BLK_KC = 16;
@@ -365,7 +367,7 @@ constexpr int BLK_P = 66;
 constexpr size_t BLK_SMEM = 2 * 2 * BLK_KC * BLK_P * sizeof(double2);
 
 template <int TC, int WR, int WC>
-__global__ void __launch_bounds__(256, 2) k_ldl_bulk(cd* __restrict__ A, int ld, int p0, int p1, int r0, int rend,
+__global__ void __launch_bounds__(256, 3) k_ldl_bulk(cd* __restrict__ A, int ld, int p0, int p1, int r0, int rend,
                                                    int c0, int n, const cd* __restrict__ vbuf, cd* __restrict__ dw)
 {
     constexpr int MT = LDL_NB / WR / 8;  // 8 x 8 tiles per warp along rows
@@ -407,22 +409,6 @@ __global__ void __launch_bounds__(256, 2) k_ldl_bulk(cd* __restrict__ A, int ld,
     };
     const int nch = (b + BLK_KC - 1) / BLK_KC;
     stage(0, 0);
-    // the tile's current values, loaded while the first chunk streams in
-    double2 old[MT][NT][2];
-#pragma unroll
-    for (int mt = 0; mt < MT; mt++)
-#pragma unroll
-        for (int nt = 0; nt < NT; nt++)
-#pragma unroll
-            for (int e = 0; e < 2; e++) {
-                const int r = rb + (wr * MT + mt) * 8 + g;
-                const int c = cb + (wc * NT + nt) * 8 + t4 * 2 + e;
-                double2 v = make_double2(0.0, 0.0);
-                if (r < rend && c < n && c >= r)
-                    v = (c == r) ? *reinterpret_cast<const double2*>(dw + c)
-                                 : *reinterpret_cast<const double2*>(A + (size_t)r + (size_t)c * ld);
-                old[mt][nt][e] = v;
-            }
     for (int ch = 0; ch < nch; ch++) {
         if (ch + 1 < nch) {
             stage(ch + 1, (ch + 1) & 1);
@@ -463,7 +449,8 @@ __global__ void __launch_bounds__(256, 2) k_ldl_bulk(cd* __restrict__ A, int ld,
                 const int c = cb + (wc * NT + nt) * 8 + t4 * 2 + e;
                 if (r >= rend || c >= n || c < r) continue;
                 const double vr = accr[mt][nt][e], vi = acci[mt][nt][e];
-                const double2 o = old[mt][nt][e];
+                const double2 o = (c == r) ? *reinterpret_cast<const double2*>(dw + c)
+                                           : *reinterpret_cast<const double2*>(A + (size_t)r + (size_t)c * ld);
                 if (c == r)
                     *reinterpret_cast<double2*>(dw + c) = make_double2(o.x - vr, o.y + vi);
                 else
