@@ -109,7 +109,13 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv")
+        # the raw samples go to ECG_BENCH_CLOCKS_DIR when it is set, else to a temporary file
+        out = os.environ.get("ECG_BENCH_CLOCKS_DIR")
+        if out:
+            self.path = os.path.join(out, f"clocks_rank{device}.csv")
+        else:
+            import tempfile
+            self.path = os.path.join(tempfile.gettempdir(), f"ecg_bench_clocks_{os.getpid()}_{device}.csv")
 
     def start(self):
         try:
