@@ -678,6 +678,28 @@ int ecg_energy_ga(ecg_ctx* ctx, int nmin, int nmax, int mat_elem_needed, int whi
     return r;
 }
 
+int ecg_energy_gb(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, int which, double* energy, double* grad_host)
+{
+    if (!ctx || !energy) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (c.method != 'G' || nfru < 0 || nfa <= nfru || nfa > c.ld) return ECG_EARG;
+    if (nfa - nfru > c.max_nfo) return ECG_EARG;
+    if (!mat_elem_needed && !c.D) return ECG_EARG;  // Glob_D is formed by the first derivative pass
+    if (cudaSetDevice(c.dev) != cudaSuccess) return ECG_ECUDA;
+    if (mat_elem_needed) CKR(compute_hsd(c, nfru + 1, nfa, nfru, 0.0));
+    const int r = energy_ga(c, nfru + 1, nfa, 0, which, 1, energy);
+    if (r != ECG_OK) return r;
+    const int nfo = nfa - nfru;
+    CKR(launch_plain_contract(c, nfo, nfa, nfru, *energy));
+    if (grad_host) {
+        CK(cudaMemcpyAsync(grad_host, c.grad, (size_t)nfo * c.npt * sizeof(double), cudaMemcpyDeviceToHost,
+                           c.stream));
+        c.bytes_d2h += (long long)nfo * c.npt * sizeof(double);
+    }
+    CK(cudaStreamSynchronize(c.stream));
+    return ECG_OK;
+}
+
 int ecg_energy_gb_adjoint(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, int which, double* energy,
                           double* grad_host)
 {

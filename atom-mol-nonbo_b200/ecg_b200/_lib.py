@@ -30,6 +30,7 @@ PROTOTYPES = {
     "ecg_eval_candidates": (C.c_int, [_vp, C.c_int, C.c_int, _dp, C.c_double, C.c_double, C.c_int, _dp, _ip, _ip,
                                       _dp]),
     "ecg_energy_ga": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _ip]),
+    "ecg_energy_gb": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]),
     "ecg_energy_gb_adjoint": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]),
     "ecg_overlap_penalty": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _dp, _dp]),
     "ecg_expectation_values": (C.c_int, [_vp, C.c_int, _dp, C.c_int, C.c_int, _ip, _ip, C.c_double, _dp, C.c_int,

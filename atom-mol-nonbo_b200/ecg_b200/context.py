@@ -193,6 +193,16 @@ class Context:
                                             int(bool(want_vector)), C.byref(e), C.byref(nf)), "ecg_energy_ga")
         return e.value, err, nf.value
 
+    def energy_gb(self, nfru, nfa, which=1, mat_elem_needed=True):
+        """EnergyGB (src/workproc.f90:1841-1950), plain drop-in: Glob_D
+        formed by ComputeMatElemAndDeriv, then contracted.  Needs a 'G'
+        context with max_nfo >= nfa - nfru.  Returns (E, gradient, ErrorCode)."""
+        e = C.c_double()
+        g = np.zeros((nfa - nfru) * self.npt)
+        err = _check(self.lib.ecg_energy_gb(self.h, int(nfru), int(nfa), int(bool(mat_elem_needed)), int(which),
+                                            C.byref(e), dptr(g)), "ecg_energy_gb")
+        return e.value, g, err
+
     def energy_gb_adjoint(self, nfru, nfa, which=1, mat_elem_needed=True):
         """EnergyGB (src/workproc.f90:1841-1950) through the fused adjoint
         pass.  Returns (E, gradient, ErrorCode)."""

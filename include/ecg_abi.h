@@ -139,6 +139,13 @@ int ecg_eval_candidates(ecg_ctx* ctx, int nbase, int count, const double* cand_h
 int ecg_energy_ga(ecg_ctx* ctx, int nmin, int nmax, int mat_elem_needed, int which, int want_vector, double* energy,
                   int* num_factorizations);
 
+/* EnergyGB, src/workproc.f90:1841-1950 (plain drop-in, contexts created
+ * with method 'G' and max_nfo >= nfa - nfru): optional
+ * ComputeMatElemAndDeriv(nfru+1, nfa), EnergyGAM's eigenpair (Glob_c with
+ * c^H S c = 1), then the gradient contraction over Glob_D
+ * (src/workproc.f90:1927-1940).  grad_host as for ecg_energy_ib. */
+int ecg_energy_gb(ecg_ctx* ctx, int nfru, int nfa, int mat_elem_needed, int which, double* energy, double* grad_host);
+
 /* EnergyGB, src/workproc.f90:1841-1950, through the fused adjoint pass:
  * optional ComputeMatElem(nfru+1, nfa), EnergyGAM's eigenpair, then the
  * gradient of ecg_energy_ib_adjoint (same ordering) at that eigenpair. */

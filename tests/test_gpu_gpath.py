@@ -106,3 +106,21 @@ def test_gb_gradient_matches_i_path(which):
     print(f"which={which}: E_G={Eg:.15f} E_I={Ei:.15f} max rel grad diff {d:.2e}")
     assert abs(Eg - Ei) <= TOL_E
     assert d <= 1e-7
+
+
+@pytest.mark.parametrize("nfru", [0, 30])
+def test_gb_plain_matches_adjoint(nfru):
+    """EnergyGB through Glob_D (ecg_energy_gb) and through the fused adjoint
+    pass: same eigenvalue, gradients within 1e-9 of the largest entry."""
+    sysm, params = synth.config_basis(1, K=90)
+    K = 90
+    with Context(sysm, K, max_nfo=K, method="G") as ctx:
+        ctx.set_params(params)
+        ctx.compute_mat_elem(1, K, 0.0)
+        Ep, gp, errp = ctx.energy_gb(nfru, K, which=1)
+        Ea, ga, erra = ctx.energy_gb_adjoint(nfru, K, which=1)
+    d = np.max(np.abs(gp - ga)) / np.max(np.abs(ga))
+    print(f"nfru={nfru}: E plain {Ep:.15f} adjoint {Ea:.15f}, max rel grad diff {d:.2e}")
+    assert errp == 0 and erra == 0
+    assert abs(Ep - Ea) <= 1e-12 * abs(Ea)
+    assert d <= 1e-9
