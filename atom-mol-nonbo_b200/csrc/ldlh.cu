@@ -358,20 +358,25 @@ __global__ void __launch_bounds__(256) k_ldl_trsm(cd* __restrict__ A, int ld, in
 // values stay interleaved in shared memory with a pitch of 66 double2
 // (= 2 mod 8 slots of 16 B), so the fragment loads of a warp are
 // conflict-free.  The tile's old values are read after the products (kept
-// out of registers during them, so three CTAs fit on an SM).
-// <64, 2, 4>: the bulk (64 x 64 tiles, side stream);
-// <16, 8, 1>: the rows of the next panel (64 x 16 tiles, enough CTAs for one
-// row of tiles, main stream).
+// out of registers during them).  <32, 4, 2>: the bulk (64 x 32 tiles, side
+// stream; at 64 registers four CTAs fit on an SM, which measured faster
+// than 64 x 64 tiles at three); <16, 8, 1>: the rows of the next panel
+// (64 x 16 tiles, enough CTAs for one row of tiles, main stream).
 constexpr int BLK_KC = 16;
 constexpr int BLK_P = 66;
-constexpr size_t BLK_SMEM = 2 * 2 * BLK_KC * BLK_P * sizeof(double2);
+// pitch of the Wun buffer: TC + 2 double2 (also = 2 mod 8), 66 for TC = 64
+template <int TC>
+__host__ __device__ constexpr int blk_vp() { return TC == 64 ? BLK_P : TC + 2; }
+template <int TC>
+constexpr size_t blk_smem() { return (size_t)2 * BLK_KC * (BLK_P + blk_vp<TC>()) * sizeof(double2); }
 
 template <int TC, int WR, int WC>
-__global__ void __launch_bounds__(256, 3) k_ldl_bulk(cd* __restrict__ A, int ld, int p0, int p1, int r0, int rend,
+__global__ void __launch_bounds__(256, TC == 64 ? 3 : 4) k_ldl_bulk(cd* __restrict__ A, int ld, int p0, int p1, int r0, int rend,
                                                    int c0, int n, const cd* __restrict__ vbuf, cd* __restrict__ dw)
 {
     constexpr int MT = LDL_NB / WR / 8;  // 8 x 8 tiles per warp along rows
     constexpr int NT = TC / WC / 8;      // and along columns
+    constexpr int VP = blk_vp<TC>();
     extern __shared__ double2 sb[];
     const int rb = r0 + blockIdx.y * LDL_NB;
     const int cb = c0 + blockIdx.x * TC;
@@ -389,7 +394,7 @@ __global__ void __launch_bounds__(256, 3) k_ldl_bulk(cd* __restrict__ A, int ld,
             for (int e = 0; e < 2; e++) accr[mt][nt][e] = acci[mt][nt][e] = 0.0;
     auto stage = [&](int ch, int buf) {
         const int k0 = ch * BLK_KC;
-        double2* Us = sb + buf * 2 * BLK_KC * BLK_P;
+        double2* Us = sb + buf * BLK_KC * (BLK_P + VP);
         double2* Vs = Us + BLK_KC * BLK_P;
         for (int e = tid; e < BLK_KC * LDL_NB; e += 256) {
             const int q = e % BLK_KC, mm = e / BLK_KC;
@@ -402,7 +407,7 @@ __global__ void __launch_bounds__(256, 3) k_ldl_bulk(cd* __restrict__ A, int ld,
             const int q = e % BLK_KC, mm = e / BLK_KC;
             const int c = cb + mm;
             const bool kv = (k0 + q < b) && (c < n);
-            cp_async16(Vs + q * BLK_P + mm,
+            cp_async16(Vs + q * VP + mm,
                        kv ? (const void*)(vbuf + (size_t)(k0 + q) + (size_t)c * LDL_NB) : (const void*)vbuf, kv ? 16 : 0);
         }
         cp_async_commit();
@@ -417,7 +422,7 @@ __global__ void __launch_bounds__(256, 3) k_ldl_bulk(cd* __restrict__ A, int ld,
             cp_async_wait<0>();
         }
         __syncthreads();
-        const double2* Us = sb + (ch & 1) * 2 * BLK_KC * BLK_P;
+        const double2* Us = sb + (ch & 1) * BLK_KC * (BLK_P + VP);
         const double2* Vs = Us + BLK_KC * BLK_P;
 #pragma unroll
         for (int kk = 0; kk < BLK_KC; kk += 4) {
@@ -426,7 +431,7 @@ __global__ void __launch_bounds__(256, 3) k_ldl_bulk(cd* __restrict__ A, int ld,
 #pragma unroll
             for (int mt = 0; mt < MT; mt++) a[mt] = Us[kr + (wr * MT + mt) * 8 + g];
 #pragma unroll
-            for (int nt = 0; nt < NT; nt++) v[nt] = Vs[kr + (wc * NT + nt) * 8 + g];
+            for (int nt = 0; nt < NT; nt++) v[nt] = Vs[(kk + t4) * VP + (wc * NT + nt) * 8 + g];
 #pragma unroll
             for (int mt = 0; mt < MT; mt++)
 #pragma unroll
@@ -470,10 +475,10 @@ static void launch_update(Ctx& c, cudaStream_t st, const cd* vb, int p0, int p1,
         // one panel of rows (the lookahead rows): narrow 64 x 16 tiles so
         // that enough CTAs run
         dim3 g((n - c0 + 15) / 16, 1);
-        k_ldl_bulk<16, 8, 1><<<g, 256, BLK_SMEM, st>>>(c.F, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
+        k_ldl_bulk<16, 8, 1><<<g, 256, blk_smem<16>(), st>>>(c.F, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
     } else {
-        dim3 g((n - c0 + LDL_NB - 1) / LDL_NB, nrb);
-        k_ldl_bulk<64, 2, 4><<<g, 256, BLK_SMEM, st>>>(c.F, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
+        dim3 g((n - c0 + 31) / 32, nrb);
+        k_ldl_bulk<32, 4, 2><<<g, 256, blk_smem<32>(), st>>>(c.F, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
     }
     c.launches++;
 }
@@ -553,8 +558,8 @@ int ldlh_factor(Ctx& c, int m0, int n)
         cudaFuncSetAttribute(k_ldl_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
         cudaFuncSetAttribute(k_ldl_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DG_SMEM);
         cudaFuncSetAttribute(k_ldl_linv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * sm1));
-        cudaFuncSetAttribute(k_ldl_bulk<64, 2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BLK_SMEM);
-        cudaFuncSetAttribute(k_ldl_bulk<16, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BLK_SMEM);
+        cudaFuncSetAttribute(k_ldl_bulk<32, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem<32>());
+        cudaFuncSetAttribute(k_ldl_bulk<16, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem<16>());
         g_ldl_attr = true;
     }
     // block list: existing blocks truncated at m0, then new 64-row blocks
