@@ -564,6 +564,15 @@ int ecg_set_params(ecg_ctx* ctx, const double* params_host, int first, int count
     return ECG_OK;
 }
 
+int ecg_set_params_device(ecg_ctx* ctx, const double* params_dev, int first, int count)
+{
+    if (!ctx || !params_dev || first < 1 || count < 0 || first - 1 + count > ctx->c.ld) return ECG_EARG;
+    Ctx& c = ctx->c;
+    CK(cudaMemcpyAsync(c.params + (size_t)(first - 1) * c.npt, params_dev, (size_t)count * c.npt * sizeof(double),
+                       cudaMemcpyDeviceToDevice, c.stream));
+    return ECG_OK;
+}
+
 int ecg_compute_mat_elem(ecg_ctx* ctx, int nmin, int nmax, double approx_energy)
 {
     if (!ctx) return ECG_EARG;

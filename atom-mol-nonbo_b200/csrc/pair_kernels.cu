@@ -1060,7 +1060,10 @@ int launch_cand_rows(Ctx& c, CandWork& cw, int nbase, int count, double approx_e
 // library holds the array (about 4.3 MB) until the process exits.  All calls
 // on a device share the array, so calls whose GPU work overlaps (different
 // streams, other host threads) race on it; each call rewrites every part of
-// it that the call reads, so nothing has to start at zero.
+// it that the call reads, so nothing has to start at zero.  The projector
+// terms reach the array through the arguments of a small kernel (copied at
+// launch), so the call issues no host-to-device copy and does not wait for
+// the stream.
 // ---------------------------------------------------------------------------
 #include <mutex>
 #include "../../include/ecg_abi.h"
@@ -1093,8 +1096,8 @@ static std::mutex g_mu;
 static unsigned char* g_base[MAX_DEVICES] = {};
 
 // Device address of g_scratch on the current device, looked up once per
-// device (the first call on a device does it; that first call should come
-// before any stream capture).
+// device: the first call on a device does this set-up, so that first call
+// should come before any stream capture on the device.
 static int device_base(unsigned char** out)
 {
     int dev = 0;
@@ -1115,13 +1118,27 @@ static int device_base(unsigned char** out)
     return ECG_OK;
 }
 
+// Projector terms by value (row-major P[t][i][j], then the coefficients):
+// 16 * 25 + 16 doubles, well inside the kernel-parameter limit.
+struct Terms {
+    double P[TMAXN * NMAX * NMAX];
+    double coef[TMAXN];
+};
+
+__global__ void k_store_terms(const Terms t, int nterms, double* __restrict__ P, double* __restrict__ coef)
+{
+    for (int e = threadIdx.x; e < nterms * NMAX * NMAX; e += blockDim.x) P[e] = t.P[e];
+    for (int e = threadIdx.x; e < nterms; e += blockDim.x) coef[e] = t.coef[e];
+}
+
 template <int N>
-static int run(const SysParams& sp, unsigned char* base, const double* params, const cd* cvec, const double* diagS,
+static int run(const SysParams& sp, const Terms& terms, unsigned char* base, const double* params, const cd* cvec, const double* diagS,
                double E, int nfru, int nfa, double* grad, cudaStream_t st)
 {
     constexpr int NV = AdjNV<N>::value;
     double* Pd = reinterpret_cast<double*>(base + OFF_P);
     double* coef = reinterpret_cast<double*>(base + OFF_COEF);
+    k_store_terms<<<1, 128, 0, st>>>(terms, sp.T, Pd, coef);
     cd* bra = reinterpret_cast<cd*>(base + OFF_BRA);
     cd* ket = reinterpret_cast<cd*>(base + OFF_KET);
     double* detL = reinterpret_cast<double*>(base + OFF_DET);
@@ -1130,8 +1147,10 @@ static int run(const SysParams& sp, unsigned char* base, const double* params, c
     const int Rlo = nfru / TILE, Rhi = (nfa + TILE - 1) / TILE;
     const long long nt = tile_count(Rlo, Rhi);
     const size_t smem = (size_t)8 * TILE * NV * sizeof(double);
-    if (cudaFuncSetAttribute(k_adjoint<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (cudaFuncSetAttribute(k_adjoint<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
         return ECG_ECUDA;
+    }
     k_adjoint<N><<<(unsigned)nt, 256, smem, st>>>(sp, coef, Pd, bra, ket, detL, diagS, cvec, E, nfru, nfa, Rlo, part);
     const int nf = nfa - nfru;
     k_adjoint_final<N><<<(nf * 32 + 255) / 256, 256, 0, st>>>(part, params, nfru, nfa, Rlo, Rhi, grad);
@@ -1152,6 +1171,7 @@ extern "C" int ecg_adjoint_gradient_noalloc(int n, const double* mass_matrix_hos
         !diagS_dev || !grad_dev)
         return ECG_EARG;
     if (nfa > noalloc::KMAX || nterms > noalloc::TMAXN) return ECG_ELIMIT;
+    cudaGetLastError();  // an error left by the caller's own earlier work is not this call's
     unsigned char* base = nullptr;
     const int rb = noalloc::device_base(&base);
     if (rb != ECG_OK) return rb;
@@ -1165,27 +1185,21 @@ extern "C" int ecg_adjoint_gradient_noalloc(int n, const double* mass_matrix_hos
     sp.two_r3n2 = pow(2.0, (3 * n) / 2.0);
     sp.n = n;
     sp.T = nterms;
-    // projector terms go into the scratch array (double, row-major P[t][i][j])
-    double P[noalloc::TMAXN * NMAX * NMAX];
-    double cf[noalloc::TMAXN];
+    // projector terms (double, row-major P[t][i][j]) travel as kernel arguments
+    noalloc::Terms terms;
+    memset(&terms, 0, sizeof(terms));
     for (int t = 0; t < nterms; t++) {
         for (int i = 0; i < NMAX; i++)
             for (int j = 0; j < NMAX; j++)
-                P[(t * NMAX + i) * NMAX + j] = (i < n && j < n) ? yhy_mats_host[(size_t)t * n * n + i + j * n] : 0.0;
-        cf[t] = yhy_coeffs_host[t];
-    }
-    if (cudaMemcpyAsync(base + noalloc::OFF_P, P, sizeof(double) * nterms * NMAX * NMAX, cudaMemcpyHostToDevice, st) !=
-            cudaSuccess ||
-        cudaMemcpyAsync(base + noalloc::OFF_COEF, cf, sizeof(double) * nterms, cudaMemcpyHostToDevice, st) !=
-            cudaSuccess) {
-        cudaGetLastError();
-        return ECG_ECUDA;
+                terms.P[(t * NMAX + i) * NMAX + j] =
+                    (i < n && j < n) ? yhy_mats_host[(size_t)t * n * n + i + j * n] : 0.0;
+        terms.coef[t] = yhy_coeffs_host[t];
     }
     const cd* cv = reinterpret_cast<const cd*>(c_dev);
     switch (n) {
-        case 2: return noalloc::run<2>(sp, base, params_dev, cv, diagS_dev, energy, nfru, nfa, grad_dev, st);
-        case 3: return noalloc::run<3>(sp, base, params_dev, cv, diagS_dev, energy, nfru, nfa, grad_dev, st);
-        case 4: return noalloc::run<4>(sp, base, params_dev, cv, diagS_dev, energy, nfru, nfa, grad_dev, st);
-        default: return noalloc::run<5>(sp, base, params_dev, cv, diagS_dev, energy, nfru, nfa, grad_dev, st);
+        case 2: return noalloc::run<2>(sp, terms, base, params_dev, cv, diagS_dev, energy, nfru, nfa, grad_dev, st);
+        case 3: return noalloc::run<3>(sp, terms, base, params_dev, cv, diagS_dev, energy, nfru, nfa, grad_dev, st);
+        case 4: return noalloc::run<4>(sp, terms, base, params_dev, cv, diagS_dev, energy, nfru, nfa, grad_dev, st);
+        default: return noalloc::run<5>(sp, terms, base, params_dev, cv, diagS_dev, energy, nfru, nfa, grad_dev, st);
     }
 }

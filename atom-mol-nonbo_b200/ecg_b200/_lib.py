@@ -19,6 +19,7 @@ PROTOTYPES = {
                                  C.POINTER(_vp)]),
     "ecg_ctx_destroy": (C.c_int, [_vp]),
     "ecg_set_params": (C.c_int, [_vp, _dp, C.c_int, C.c_int]),
+    "ecg_set_params_device": (C.c_int, [_vp, C.c_void_p, C.c_int, C.c_int]),
     "ecg_compute_mat_elem": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double]),
     "ecg_compute_mat_elem_and_deriv": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_double]),
     "ecg_ghepiis": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp, _ip]),

@@ -74,6 +74,12 @@ class Context:
             raise ValueError(f"params must be (count, {self.npt})")
         _check(self.lib.ecg_set_params(self.h, dptr(p), int(first), p.shape[0]), "ecg_set_params")
 
+    def set_params_device(self, ptr, first, count):
+        """Glob_NonlinParam(:, first:first+count-1) from device memory at
+        address ptr (npt x count doubles on the context's device)."""
+        _check(self.lib.ecg_set_params_device(self.h, C.c_void_p(int(ptr)), int(first), int(count)),
+               "ecg_set_params_device")
+
     def matrices(self, n):
         H = np.zeros((n, n), dtype=np.complex128, order="F")
         S = np.zeros((n, n), dtype=np.complex128, order="F")

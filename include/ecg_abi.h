@@ -52,8 +52,14 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
                    int device, ecg_ctx** out);
 int ecg_ctx_destroy(ecg_ctx* ctx);
 
-/* Glob_NonlinParam(1:npt, first:first+count-1) = params_host (npt x count). */
+/* Glob_NonlinParam(1:npt, first:first+count-1) = params_host (npt x count).
+ * The optimisation drivers' parameter update before each evaluation, e.g.
+ * src/workproc.f90:4157-4159 (BasisEnlI) and the FullOpt1I equivalent. */
 int ecg_set_params(ecg_ctx* ctx, const double* params_host, int first, int count);
+/* The same update from device memory (params_dev: npt x count doubles on the
+ * context's device, e.g. an optimiser that keeps its iterate on the GPU);
+ * ordered on the context's stream, no host copy. */
+int ecg_set_params_device(ecg_ctx* ctx, const double* params_dev, int first, int count);
 
 /* ComputeMatElem(Nmin,Nmax) + StoreHS, src/matform.f90:119-230 and :11-51.
  * approx_energy = Glob_ApproxEnergy (lambda~).  Rows Nmin..Nmax of the
@@ -246,14 +252,16 @@ int ecg_io_bytes(ecg_ctx* ctx, long long* h2d, long long* d2h);
  * its eigenvalue, grad_dev receives npt*(nfa-nfru) doubles ordered as
  * ecg_energy_ib's gradient.  The system arguments are those of
  * ecg_ctx_create.  Work is queued on `stream` (a cudaStream_t, NULL for the
- * default stream) and the call returns without waiting for it.
+ * default stream); the call issues no host-to-device copy (the projector
+ * terms travel as kernel arguments) and returns without waiting for it.
  * Limits: nfa <= 512 and nterms <= 16, else ECG_ELIMIT and nothing runs.
  * The call allocates nothing: its working data lives in one fixed array of
  * about 4.3 MB compiled into the library, held by every GPU that loads it
- * until the process exits.  The first call on a device looks up that
- * array's device address (make that first call before any stream capture).
- * All calls on a device share the array: calls whose GPU work overlaps race
- * on it and must be serialised by the caller. */
+ * until the process exits.  The first call on a device does a one-time
+ * set-up (it looks up that array's device address): make that first call
+ * before any stream capture on the device.  All calls on a device share the
+ * array: calls whose GPU work overlaps race on it and must be serialised by
+ * the caller. */
 int ecg_adjoint_gradient_noalloc(int n, const double* mass_matrix_host, const double* charges_host, int nterms,
                                  const int* yhy_mats_host, const int* yhy_coeffs_host, const double* params_dev,
                                  const double* c_dev, const double* diagS_dev, double energy, int nfru, int nfa,

@@ -14,6 +14,9 @@
  *   ComputeMatElem            src/matform.f90:119-230
  *   ComputeMatElemAndDeriv    src/matform.f90:234-360
  *   LDLHF (serial branch)     src/linalg.f90:316-392
+ *   LDLHF (parallel branch)   src/linalg.f90:400-452, OpenMP threads as the
+ *                             ranks; chosen as linalg_setparam does,
+ *                             src/linalg.f90:113-121
  *   LDLHS (non-BLAS branch)   src/linalg.f90:618-653
  *   MHMV  (non-BLAS branch)   src/linalg.f90:1019-1043
  *   VMMHMV (serial branch)    src/linalg.f90:1180-1215
@@ -632,6 +635,30 @@ void orc_compute_mat_elem(const double *params, int nmin, int nmax, char method,
     }
 }
 
+/* For the parity tests' tolerance scales: for every pair k >= l of
+ * functions 1..K, aH = sum_t |coef_t| |H_t(k,l)| and aS likewise, as
+ * (K x K) column-major arrays (lower triangle filled).  Not a reference
+ * routine: the magnitude of the terms that ComputeMatElem sums. */
+void orc_term_magnitudes(const double *params, int K, double *aH, double *aS)
+{
+    const int npt = g_npt;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int k = 1; k <= K; k++) {
+        for (int l = 1; l <= k; l++) {
+            double h = 0.0, sm = 0.0;
+            for (int t = 0; t < g_T; t++) {
+                cplx Hkl, Skl;
+                matrix_elements(params + (size_t)(k - 1) * npt, params + (size_t)(l - 1) * npt, g_P[t], &Hkl,
+                                &Skl, 0, 0, 0);
+                h += abs(g_coef[t]) * cabs(Hkl);
+                sm += abs(g_coef[t]) * cabs(Skl);
+            }
+            aH[IX(k, l, K)] = h;
+            aS[IX(k, l, K)] = sm;
+        }
+    }
+}
+
 /* StoreHSD, matform.f90:55-115.  D is (2npt, ldo, *) column-major. */
 static void store_hsd(char method, double approx_e, int nfru, int i, int j, cplx Hij, cplx Sij,
                       const cplx *Di, const cplx *Dj, cplx *H, cplx *S, int ld, double *diagS,
@@ -698,6 +725,99 @@ int orc_ldlhf(int m, int n, cplx *A, int ld, cplx *invD, cplx *w)
         }
     }
     return 0;
+}
+
+/* LDLHF parallel branch (Glob_LDLHF_PMode /= 0), linalg.f90:400-452, with
+ * the OpenMP threads of one team as the MPI ranks (Glob_NumOfProcs = team
+ * size, Glob_ProcID = thread number).  Row i of L^H is built in chunks of
+ * NumOfProcs entries: rank r forms entry ji+r of the chunk from the part of
+ * the row before the chunk (one dot product), the chunk is gathered (the
+ * reference's MPI_ALLREDUCE over entries that only one rank set), and every
+ * entry then takes the within-chunk terms in order.  The diagonal term is a
+ * strided partial sum per rank, reduced.  A barrier stands in for each
+ * ALLREDUCE; the within-chunk steps, which every rank repeats identically
+ * in the reference, run once.  Returns ErrorCode. */
+int orc_ldlhf_par(int m, int n, cplx *A, int ld, cplx *invD, cplx *w)
+{
+    int err = 0;
+    cplx part[256];
+#pragma omp parallel
+    {
+#ifdef _OPENMP
+        const int np = omp_get_num_threads() > 256 ? 256 : omp_get_num_threads();
+        const int id = omp_get_thread_num();
+#else
+        const int np = 1, id = 0;
+#endif
+        for (int i = m; i <= n && !err; i++) {
+            const int im = i - 1;
+#pragma omp single
+            for (int q = 1; q <= im; q++) A[IX(q, i, ld)] = 0.0;
+            const int rows = im / np, rem = im % np;
+            for (int k = 1; k <= rows + (rem > 0); k++) {
+                const int ji = (k - 1) * np + 1, jim = ji - 1;
+                const int jf = (k <= rows) ? k * np : im;
+                const int jiR = ji + id;
+                if (id < np && jiR <= jf) {
+                    /* A(jiR,i) = conjg(-dot_product(A(1:jim,i), A(1:jim,jiR))) */
+                    cplx d = 0.0;
+                    for (int q = 1; q <= jim; q++) d = d + conj(A[IX(q, i, ld)]) * A[IX(q, jiR, ld)];
+                    A[IX(jiR, i, ld)] = conj(-d);
+                }
+#pragma omp barrier
+#pragma omp single
+                for (int j = ji; j <= jf; j++) {
+                    /* A(j,i) += conjg(A(i,j) - dot_product(A(ji:jm,i), A(ji:jm,j))) */
+                    cplx d = 0.0;
+                    for (int q = ji; q <= j - 1; q++) d = d + conj(A[IX(q, i, ld)]) * A[IX(q, j, ld)];
+                    A[IX(j, i, ld)] = A[IX(j, i, ld)] + conj(A[IX(i, j, ld)] - d);
+                }
+            }
+            /* the j == 1 (diagonal) case */
+#pragma omp for schedule(static)
+            for (int q = 1; q <= im; q++) w[q - 1] = A[IX(q, i, ld)] * invD[q - 1];
+            cplx y = 0.0;
+            for (int q = 1 + id; q <= im; q += np) y = y + conj(A[IX(q, i, ld)]) * w[q - 1];
+            if (id < 256) part[id] = conj(y);
+#pragma omp barrier
+#pragma omp single
+            {
+                cplx x = 0.0;
+                for (int r = 0; r < np; r++) x = x + part[r];
+                x = A[IX(i, i, ld)] - x;
+                for (int q = 1; q <= im; q++) A[IX(q, i, ld)] = w[q - 1];
+                if (x == 0.0)
+                    err = 1;
+                else
+                    invD[i - 1] = 1.0 / x;
+            }
+        }
+    }
+    return err;
+}
+
+/* Which LDLHF branch GHEPIIS calls: 0 serial, 1 parallel, -1 (default) as
+ * linalg_setparam('marin') picks it for NumOfProcs = the thread count:
+ * parallel when NumOfProcs >= 8 and n > 5000 or NumOfProcs >= 16 and
+ * n > 3000 (src/linalg.f90:113-121). */
+static int g_ldlhf_mode = -1;
+
+void orc_set_ldlhf_mode(int mode) { g_ldlhf_mode = mode; }
+
+static int ldlhf_parallel(int n)
+{
+    if (g_ldlhf_mode >= 0) return g_ldlhf_mode;
+#ifdef _OPENMP
+    const int procs = omp_get_max_threads();
+#else
+    const int procs = 1;
+#endif
+    return (procs >= 8 && n > 5000) || (procs >= 16 && n > 3000);
+}
+
+int orc_ldlhf_auto(int m, int n, cplx *A, int ld, cplx *invD, cplx *w)
+{
+    return ldlhf_parallel(n) ? orc_ldlhf_par(m, n, A, ld, invD, w) : orc_ldlhf(m, n, A, ld, invD, w);
 }
 
 /* LDLHS non-BLAS branch, linalg.f90:634-653 (the BLAS branch at :655-660
@@ -802,7 +922,7 @@ int orc_ghepiis(int k, int n, cplx *M, int ldm, cplx *invD, const cplx *B, int l
     cplx tc;
     out[1] = DBL_MAX;
     iout[0] = 0;
-    err = orc_ldlhf(k, n, M, ldm, invD, w);
+    err = orc_ldlhf_auto(k, n, M, ldm, invD, w);
     if (err > 0) return err;
     sqrtn = sqrt(2 * n * 1.0);
     while (notconverged && NumIter < maxiter) {

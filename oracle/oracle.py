@@ -43,6 +43,10 @@ def load():
                                                        _dp, C.c_int, _dp, _dp, _dp, C.c_int]
         lib.orc_ldlhf.argtypes = [C.c_int, C.c_int, _dp, C.c_int, _dp, _dp]
         lib.orc_ldlhf.restype = C.c_int
+        lib.orc_ldlhf_par.argtypes = [C.c_int, C.c_int, _dp, C.c_int, _dp, _dp]
+        lib.orc_ldlhf_par.restype = C.c_int
+        lib.orc_set_ldlhf_mode.argtypes = [C.c_int]
+        lib.orc_term_magnitudes.argtypes = [_dp, C.c_int, _dp, _dp]
         lib.orc_ldlhs.argtypes = [C.c_int, _dp, C.c_int, _dp, _dp, _dp]
         lib.orc_vmmhmv.argtypes = [C.c_int, _dp, C.c_int, _dp]
         lib.orc_vmmhmv.restype = C.c_double
@@ -76,6 +80,13 @@ def set_threads(n):
 
 def get_threads():
     return load().orc_get_threads()
+
+
+def set_ldlhf_mode(mode):
+    """LDLHF branch used by GHEPIIS: 0 serial, 1 parallel (the threads act
+    as the MPI ranks), -1 as linalg_setparam picks it for the thread count
+    (src/linalg.f90:113-121)."""
+    load().orc_set_ldlhf_mode(int(mode))
 
 
 class Oracle:
@@ -122,6 +133,14 @@ class Oracle:
         dl = np.zeros(4 * self.np, dtype=np.complex128)
         self.lib.orc_matrix_elements(_p(pk), _p(pl), Pcm.ctypes.data_as(_ip), _p(hs), _p(dk), _p(dl), gradflag)
         return hs[0], hs[1], dk, dl
+
+    def term_magnitudes(self, K):
+        """(aH, aS): for k >= l, sum over the Y^+Y terms of |coef| |H_t(k,l)|
+        and |coef| |S_t(k,l)| (lower triangles of K x K arrays)."""
+        aH = np.zeros((K, K), order="F")
+        aS = np.zeros((K, K), order="F")
+        self.lib.orc_term_magnitudes(_p(self.params), K, _p(aH), _p(aS))
+        return aH, aS
 
     def compute_mat_elem(self, nmin, nmax, approx_e, method="I"):
         self.lib.orc_compute_mat_elem(_p(self.params), nmin, nmax, method.encode(), approx_e, _p(self.H), _p(self.S),

@@ -9,15 +9,15 @@ stored CURRENT_ENERGY, WHICH_EIGENVALUE, INVITPARAMETER, EIGVAL_TOLERANCE and
 the K x npt nonlinear parameters in hdplus_fixtures.npz, and copies one of
 the files (inout_2_500.txt) unchanged for the data-file reader/writer tests.
 
-Run it in a checkout that has the reference at REFERENCE_ROOT (default
-/root/reference).  The GPU tests only read the .npz it writes.
+Run it with REFERENCE_ROOT set to the root of a checkout of the reference
+(the folder holding example_input/).  The tests only read the .npz it writes.
 """
 import os
 import sys
 
 import numpy as np
 
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("REFERENCE_ROOT")
 HERE = os.path.dirname(os.path.abspath(__file__))
 NAMES = [f"inout_{w}_{k}" for w in (1, 2) for k in (500, 1000, 1500)]
 TEXT_FIXTURE = "inout_2_500"
@@ -58,6 +58,9 @@ def read_inout(path):
 
 
 def main():
+    if not REF:
+        print("set REFERENCE_ROOT to the reference checkout (the folder holding example_input/)", file=sys.stderr)
+        return 2
     out = {}
     for name in NAMES:
         d = read_inout(os.path.join(REF, "example_input", name + ".txt"))

@@ -76,3 +76,46 @@ def tolerance(kappa, rtol=1e-12, c=64.0):
     1e-12, or c * eps * kappa when the element is worse conditioned (both
     evaluations then carry errors of a few eps * kappa)."""
     return np.maximum(rtol, c * EPS * np.asarray(kappa))
+
+
+def pair_conditions_at(sysm, params, kk, ll):
+    """pair_conditions for the listed pairs only (arrays of 0-based k, l)."""
+    kk = np.asarray(kk)
+    ll = np.asarray(ll)
+    kap = np.zeros(kk.size)
+    for a, b in ((kk, ll), (kk, kk), (ll, ll)):
+        for t in range(sysm.T):
+            kap = np.maximum(kap, term_conditions(sysm, params[a], params[b], np.full(a.size, t)))
+    return kap
+
+
+def hs_ratio(o, sysm, params, K, lam, method, H, S, dS):
+    """Largest |GPU - oracle| / (scale * tolerance) over every stored element
+    of H, S (lower triangle; strict in 'G' storage) and diagS.  scale is the
+    sum over Y^+Y terms of |coef| |term| as stored (terms of opposite sign
+    cancel), plus |lambda~| times that of S for 'I' storage's H - lambda~ S;
+    tolerance is 1e-12, or 64 eps cond(C) for the elements where that is
+    larger (cond(C) evaluated only where an element is beyond 1e-12)."""
+    lo = np.tril_indices(K, -1 if method == "G" else 0)
+    aH, aS = o.term_magnitudes(K)
+    f = 1.0 / np.sqrt(np.outer(o.diagS[:K], o.diagS[:K]))
+    sH = ((aH + (abs(lam) * aS if method == "I" else 0.0)) * f)[lo]
+    sS = (aS * f)[lo]
+    dH = np.abs(H[lo] - o.H[:K, :K][lo]) / sH
+    dSm = np.abs(S[lo] - o.S[:K, :K][lo]) / sS
+    out = {"H_within_1e-12": float(np.mean(dH <= 1e-12)), "S_within_1e-12": float(np.mean(dSm <= 1e-12))}
+    for name, d in (("H", dH), ("S", dSm)):
+        bad = np.nonzero(d > 1e-12)[0]
+        r = float(np.max(d)) / 1e-12 if d.size else 0.0
+        if bad.size:
+            kap = pair_conditions_at(sysm, params, lo[0][bad], lo[1][bad])
+            r = max(float(np.max(np.where(d <= 1e-12, d, 0.0))) / 1e-12, float(np.max(d[bad] / tolerance(kap))))
+        out[name] = r
+    dd = np.abs(dS - o.diagS[:K]) / np.abs(o.diagS[:K])
+    bad = np.nonzero(dd > 1e-12)[0]
+    rd = float(np.max(dd)) / 1e-12
+    if bad.size:
+        kap = pair_conditions_at(sysm, params, bad, bad)
+        rd = max(float(np.max(np.where(dd <= 1e-12, dd, 0.0))) / 1e-12, float(np.max(dd[bad] / tolerance(kap))))
+    out["diagS"] = rd
+    return out

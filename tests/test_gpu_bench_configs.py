@@ -1,0 +1,138 @@
+"""Parity at the sizes the benchmark configurations are quoted on, against
+the oracle:
+
+* configuration 0 (n = 2, T = 2, K = 500) and configuration 1 (n = 3,
+  T = 4, K = 1500): every stored element of H, S and diagS in the 'I' and
+  'G' layouts (ComputeMatElem + StoreHS, src/matform.f90:11-51,119-230);
+* configuration 1 at K = 1500: the energy of EnergyIAM (src/workproc.f90:
+  2010-2060) to 1e-10 hartree;
+* configuration 2 at K = 4000 (the benchmark workload): the energy and the
+  whole gradient of EnergyIB (src/workproc.f90:2063-2154), plain and fused
+  adjoint forms, against one full oracle EnergyIB (1e-10 hartree; 1e-8 of
+  the largest gradient entry), and the gradient against central finite
+  differences with h = 1e-6 (relative) on 64 seeded parameters (the
+  reference's own check, commented out at src/workproc.f90:4174-4203);
+* the energy stored for the benchmark (tests/golden/bench_k4000.json)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as orc
+from ecg_b200 import Context, synth
+from gpu_util import hs_ratio, problem
+
+pytestmark = pytest.mark.gpu
+TOL_E = 1e-10
+TOL_G = 1e-8
+FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "bench_k4000.json")
+
+
+def _gerr(g, go):
+    return float(np.max(np.abs(g - go)) / np.max(np.abs(go)))
+
+
+@pytest.mark.parametrize("cfg,K", [(0, 500), (1, 1500)])
+@pytest.mark.parametrize("method", ["I", "G"])
+def test_hs_at_configuration_size(cfg, K, method):
+    sysm, params = synth.config_basis(cfg, K=K)
+    lam = -0.55 if cfg == 0 else -1.1
+    o = orc.Oracle(sysm, K)
+    o.set_params(params)
+    o.compute_mat_elem(1, K, lam, method=method)
+    with Context(sysm, K, method=method) as ctx:
+        ctx.set_params(params)
+        ctx.compute_mat_elem(1, K, lam)
+        H, S, dS, dH, _ = ctx.matrices(K)
+    r = hs_ratio(o, sysm, params, K, lam, method, H, S, dS)
+    if method == "G":
+        dd = np.max(np.abs(dH - o.diagH[:K]) / np.maximum(np.abs(o.diagH[:K]), 1e-300))
+        r["diagH_rel"] = float(dd)
+        assert dd <= 1e-10
+    print(f"cfg {cfg} K {K} {method}: {r}")
+    assert r["H"] <= 1 and r["S"] <= 1 and r["diagS"] <= 1
+
+
+def test_energy_configuration_1():
+    K = 1500
+    sysm, params, lam, o = problem(1, K)
+    o.last[:K] = 1.0
+    Eo, erro, ito = o.energy_ia(1, K, lam, 1e-12, specif_norm=0)
+    with Context(sysm, K) as ctx:
+        ctx.set_params(params)
+        ctx.set_vectors(K, last_eigvec=np.ones(K, dtype=np.complex128))
+        E, err, it = ctx.energy_ia(1, K, lam, 1e-12, specif_norm=0)
+    print(f"K {K}: E_gpu {E:.15f} E_oracle {Eo:.15f} dE {E - Eo:.2e} codes {err}/{erro} iters {it}/{ito}")
+    assert err == 0 and abs(E - Eo) <= TOL_E
+
+
+@pytest.fixture(scope="module")
+def k4000():
+    fx = json.load(open(FIXTURE))
+    K = fx["K"]
+    sysm, params = synth.config_basis(fx["config"], K=K)
+    return fx, sysm, params
+
+
+def test_stored_benchmark_energy(k4000):
+    fx, sysm, params = k4000
+    K, lam = fx["K"], fx["lambda_tilde"]
+    with Context(sysm, K) as ctx:
+        ctx.set_params(params)
+        ctx.set_vectors(K, last_eigvec=np.ones(K, dtype=np.complex128))
+        E, err, it = ctx.energy_ia(1, K, lam, 1e-12, specif_norm=0)
+    print(f"K {K}: E_gpu {E:.15f} stored oracle {fx['energy_oracle']:.15f} dE {E - fx['energy_oracle']:.2e}")
+    assert err == 0 and abs(E - fx["energy_oracle"]) <= TOL_E
+
+
+def test_energy_and_gradient_configuration_2(k4000):
+    fx, sysm, params = k4000
+    K, lam = fx["K"], fx["lambda_tilde"]
+    o = orc.Oracle(sysm, K, max_nfo=K)
+    o.set_params(params)
+    o.last[:K] = 1.0
+    Eo, go, erro, ito = o.energy_ib(0, K, lam, 1e-12)
+    del o
+    with Context(sysm, K, max_nfo=K) as ctx:
+        ctx.set_params(params)
+        for mode in ("adjoint", "plain"):
+            ctx.set_vectors(K, last_eigvec=np.ones(K, dtype=np.complex128))
+            fn = ctx.energy_ib_adjoint if mode == "adjoint" else ctx.energy_ib
+            E, g, err, it = fn(0, K, lam, 1e-12)
+            print(f"K {K} {mode}: dE {E - Eo:.2e} grad err {_gerr(g, go):.2e} codes {err}/{erro} iters {it}/{ito}")
+            assert err == 0 and abs(E - Eo) <= TOL_E
+            assert _gerr(g, go) <= TOL_G
+
+
+def test_gradient_finite_differences_configuration_2(k4000):
+    fx, sysm, params = k4000
+    K, lam = fx["K"], fx["lambda_tilde"]
+    rng = np.random.default_rng(64)
+    flat = rng.choice(K * sysm.npt, size=64, replace=False)
+    worst = 0.0
+    with Context(sysm, K) as ctx:
+        ctx.set_params(params)
+        ctx.set_vectors(K, last_eigvec=np.ones(K, dtype=np.complex128))
+        E, g, err, _ = ctx.energy_ib_adjoint(0, K, lam, 1e-12)
+        assert err == 0
+        _, x0 = ctx.vectors(K)
+        gmax = np.max(np.abs(g))
+        for idx in flat:
+            f, m = divmod(int(idx), sysm.npt)
+            h = 1e-6 * abs(params[f, m])
+            es = []
+            for s in (1, -1):
+                p2 = params[f:f + 1].copy()
+                p2[0, m] += s * h
+                ctx.set_params(p2, first=f + 1)
+                ctx.set_vectors(K, last_eigvec=x0)
+                e2, err2, _ = ctx.energy_ia(1, K, lam, 1e-12, max_iter=30)
+                assert err2 == 0
+                es.append(e2)
+            ctx.set_params(params[f:f + 1], first=f + 1)
+            fd = (es[0] - es[1]) / (2 * h)
+            an = g[idx]
+            worst = max(worst, abs(fd - an) / (1e-6 * gmax + 1e-5 * abs(an)))
+            assert abs(fd - an) <= 1e-6 * gmax + 1e-5 * abs(an), (f, m, an, fd)
+    print(f"64 parameters: worst |fd - analytic| / bound = {worst:.3f}")
