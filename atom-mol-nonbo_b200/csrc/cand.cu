@@ -745,6 +745,9 @@ int ensure_work(Ctx& c, int count)
     r |= dalloc_n(&cw.flags, (size_t)cw.nflags);
     r |= dalloc_n(&cw.bstart, (size_t)maxpanels + 1);
     r |= dalloc_n(&cw.abort_word, 1);
+    cw.gpart_n = (size_t)bcap * (c.ld / 128 + 2) * (2 * c.np + 1);
+    r |= dalloc_n(&cw.gpart, cw.gpart_n);
+    r |= dalloc_n(&cw.grad, (size_t)c.npt * bcap);
     if (!r) {
         if (cudaMallocHost((void**)&cw.st_h, sizeof(int) * (3 * (size_t)ccap + 1)) != cudaSuccess ||
             cudaMallocHost((void**)&cw.nd_h, sizeof(double) * 5 * (size_t)ccap) != cudaSuccess ||
@@ -953,7 +956,7 @@ void cand_free(CandWork& cw)
     drop_graphs(cw);
     void* ptrs[] = {cw.par, cw.bra, cw.ket, cw.det, cw.dS, cw.mu, cw.Mcol, cw.Scol, cw.Acol, cw.Lcol, cw.V, cw.W,
                     cw.Y, cw.Z, cw.X, cw.X2, cw.brd, cw.nd, cw.st, cw.cmap, cw.Gm, cw.Pk, cw.flags, cw.bstart,
-                    cw.abort_word};
+                    cw.abort_word, cw.gpart, cw.grad};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (cw.st_h) cudaFreeHost(cw.st_h);
@@ -967,13 +970,16 @@ void cand_free(CandWork& cw)
     cw.solve_grid = sg;
 }
 
-// See ecg_eval_candidates in ecg_abi.h.  Returns 0 or a negative status;
-// per-candidate ErrorCodes go to errcodes.
+// See ecg_eval_candidates / ecg_eval_candidates_grad in ecg_abi.h.  Returns
+// 0 or a negative status; per-candidate ErrorCodes go to errcodes.  With
+// grad (host, npt x count), every candidate's energy gradient with respect
+// to its own parameters too (requires nbase >= 1).
 int eval_candidates(Ctx& c, int nbase, int count, const double* cand_host, double approx_e, double tol,
-                    int max_iter, double* energies, int* errcodes, int* num_iter, double* rel_acc)
+                    int max_iter, double* energies, int* errcodes, int* num_iter, double* rel_acc, double* grad)
 {
     if (c.method != 'I') return ECG_EARG;
     if (nbase < 0 || count < 1 || nbase + 1 > c.ld || max_iter < 1 || !cand_host || !energies) return ECG_EARG;
+    if (grad && nbase < 1) return ECG_EARG;
     if (ensure_work(c, count)) return ECG_ENOMEM;
     CandWork& cw = c.cand;
     const int cc = cw.ccap;
@@ -1062,6 +1068,17 @@ int eval_candidates(Ctx& c, int nbase, int count, const double* cand_host, doubl
     k_cand_rayleigh<<<count, 256, 0, c.stream>>>(cw.X, cw.X2, cw.V, cw.Scol, cw.Mcol, cw.mu, nbase, cw.ldv, cc,
                                                  cw.brd, cw.nd, cw.st, approx_e);
     c.launches++;
+    if (grad) {
+        // EnergyIB's gradient for each candidate as function nbase+1, by the
+        // fused adjoint pass over its row
+        if (launch_cand_adjoint(c, cw, nbase, count, cw.brd + (size_t)BR_V * cc, cw.nd + (size_t)ND_T1 * cc,
+                                cw.nd + (size_t)ND_E * cc, cw.st + (size_t)ST_ERR * cc, cw.grad))
+            return ECG_ECUDA;
+        if ((r = CKc(cudaMemcpyAsync(grad, cw.grad, sizeof(double) * c.npt * count, cudaMemcpyDeviceToHost,
+                                     c.stream))))
+            return r;
+        c.bytes_d2h += (long long)sizeof(double) * c.npt * count;
+    }
     if ((r = CKc(cudaMemcpyAsync(cw.st_h, cw.st, sizeof(int) * (3 * (size_t)cc + 1), cudaMemcpyDeviceToHost,
                                  c.stream))))
         return r;

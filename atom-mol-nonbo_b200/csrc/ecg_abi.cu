@@ -504,7 +504,7 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
     r |= dalloc(&c.detL, L);
     r |= dalloc(&c.dw, L);
     r |= dalloc(&c.linv, L * LDL_NB);
-    r |= dalloc(&c.vbuf, 3 * L * LDL_NB);
+    r |= dalloc(&c.vbuf, 3 * L * LDL_VLD);
     r |= dalloc(&c.status, (size_t)ST_COUNT);
     r |= dalloc(&c.red, (size_t)RD_COUNT);
     r |= dalloc(&c.counters, (size_t)4);
@@ -675,6 +675,17 @@ int ecg_eval_candidates(ecg_ctx* ctx, int nbase, int count, const double* cand_h
     if (cudaSetDevice(c.dev) != cudaSuccess) return ECG_ECUDA;
     return eval_candidates(c, nbase, count, cand_host, approx_energy, tol, max_iter, energies_host, errcodes_host,
                            num_iter_host, rel_acc_host);
+}
+
+int ecg_eval_candidates_grad(ecg_ctx* ctx, int nbase, int count, const double* cand_host, double approx_energy,
+                             double tol, int max_iter, double* energies_host, int* errcodes_host, int* num_iter_host,
+                             double* rel_acc_host, double* grad_host)
+{
+    if (!ctx || !grad_host) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.dev) != cudaSuccess) return ECG_ECUDA;
+    return eval_candidates(c, nbase, count, cand_host, approx_energy, tol, max_iter, energies_host, errcodes_host,
+                           num_iter_host, rel_acc_host, grad_host);
 }
 
 int ecg_energy_ga(ecg_ctx* ctx, int nmin, int nmax, int mat_elem_needed, int which, int want_vector, double* energy,

@@ -12,6 +12,9 @@ namespace ecg {
 constexpr int TILE = 32;
 // LDL^H block size (rows of one panel).
 constexpr int LDL_NB = 64;
+// Trailing updates apply two panels at once (rank 128); the unscaled panel
+// rows of such a pair are kept with this many rows per column.
+constexpr int LDL_VLD = 2 * LDL_NB;
 
 // Number of 32 x 32 tiles with row-tile index in [Rlo, Rhi) and column-tile
 // index 0..R (lower triangle including diagonal tiles).
@@ -68,6 +71,9 @@ struct CandWork {
     int* bstart = nullptr;   // device panel boundaries of the base factor
     int* bstart_h = nullptr; // pinned staging
     int* abort_word = nullptr;
+    double* gpart = nullptr;  // candidate gradients: per (candidate, 128-row chunk) adjoint sums
+    size_t gpart_n = 0;
+    double* grad = nullptr;   // npt x bcap candidate gradients
     int solve_grid = 0;      // co-resident CTAs of the solve kernel
     int row_variant = -1;    // autotuned k_cand_row shape
     int tuned_n = 0, tuned_T = 0;
@@ -124,7 +130,7 @@ struct Ctx {
     // LDL^H workspace
     cd* dw = nullptr;           // working diagonal (ld)
     cd* linv = nullptr;         // ld x LDL_NB: inverse unit-lower diagonal blocks
-    cd* vbuf = nullptr;         // 3 x LDL_NB x ld: unscaled panel rows (rotating)
+    cd* vbuf = nullptr;         // 3 x LDL_VLD x ld: unscaled rows of panel pairs (rotating)
     int* status = nullptr;      // device status words (see ST_*)
     int* status_h = nullptr;    // pinned host mirror
     double* red = nullptr;      // reduction scratch for the solver (doubles)
@@ -196,13 +202,18 @@ int launch_term_batch(Ctx& c, int count, const double* pk, const double* pl, con
                       cd* hs, cd* dk, cd* dl);
 
 int launch_cand_rows(Ctx& c, CandWork& cw, int nbase, int count, double approx_e, int variant);
+// Gradients of the candidates' energies with respect to their own
+// parameters from their final eigenpairs (border entry vK, x^H S x = t1).
+int launch_cand_adjoint(Ctx& c, CandWork& cw, int nbase, int count, const cd* vK, const double* t1,
+                        const double* energy, const int* err, double* grad);
 // overlap penalty: part receives one partial sum per function nfru..nfa-1;
 // mode 0 value only, 1 adds the reference's gradient to c.grad, 2 the exact one
 int launch_penalty(Ctx& c, int nfru, int nfa, double t2, double pc, int mode, double* part);
 
 // ---- batched candidates (cand.cu) ----
 int eval_candidates(Ctx& c, int nbase, int count, const double* cand_host, double approx_e, double tol,
-                    int max_iter, double* energies, int* errcodes, int* num_iter, double* rel_acc);
+                    int max_iter, double* energies, int* errcodes, int* num_iter, double* rel_acc,
+                    double* grad = nullptr);
 void cand_free(CandWork& cw);
 
 // ---- expectation values (expc.cu) ----

@@ -234,19 +234,25 @@ __global__ void __launch_bounds__(256) k_fwd_coop(const cd* __restrict__ A, int 
     for (int m = 0; m < 8; m++) acc[m] = mk(0.0, 0.0);
     bool ok = true;
     for (int a = 0; a < j; a++) {
-        if (!wait_panel(flags, a, epoch, status, abort_word, ok)) break;
         const int a0 = bstart[a], a1 = bstart[a + 1];
         const int r0 = a0 + lane, r1 = a0 + lane + 32;
+        // the factor block U(panel a, panel j) does not depend on panel a's
+        // solution: load it before waiting for that panel's flag
+        cd u0[8], u1[8];
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const int c = wp * 8 + m;
+            const cd* col = A + (size_t)(j0 + c) * ld;
+            u0[m] = (c < b && r0 < a1) ? ld2(col + r0) : mk(0.0, 0.0);
+            u1[m] = (c < b && r1 < a1) ? ld2(col + r1) : mk(0.0, 0.0);
+        }
+        if (!wait_panel(flags, a, epoch, status, abort_word, ok)) break;
         const cd y0 = (r0 < a1) ? ldcg2(y + r0) : mk(0.0, 0.0);
         const cd y1 = (r1 < a1) ? ldcg2(y + r1) : mk(0.0, 0.0);
 #pragma unroll
         for (int m = 0; m < 8; m++) {
-            const int c = wp * 8 + m;
-            if (c < b) {
-                const cd* col = A + (size_t)(j0 + c) * ld;
-                if (r0 < a1) acc[m] = cfma(conj(ld2(col + r0)), y0, acc[m]);
-                if (r1 < a1) acc[m] = cfma(conj(ld2(col + r1)), y1, acc[m]);
-            }
+            acc[m] = cfma(conj(u0[m]), y0, acc[m]);
+            acc[m] = cfma(conj(u1[m]), y1, acc[m]);
         }
     }
 #pragma unroll
@@ -306,13 +312,23 @@ __global__ void __launch_bounds__(256) k_bwd_coop(const cd* __restrict__ A, int 
     cd a0 = mk(0.0, 0.0), a1 = mk(0.0, 0.0);  // rows lane, lane + 32
     bool ok = true;
     for (int c = nb - 1; c > j; c--) {
-        if (!wait_panel(flags, c, epoch, status, abort_word, ok)) break;
         const int c0 = bstart[c], c1 = bstart[c + 1];
-        for (int col = c0 + wp; col < c1; col += 8) {
-            const cd xc = ldcg2(x + col);
+        // U(panel j, panel c) before the wait for panel c's solution
+        cd u0[8], u1[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int col = c0 + wp + 8 * i;
             const cd* u = A + (size_t)col * ld + j0;
-            if (lane < b) a0 = cfma(ld2(u + lane), xc, a0);
-            if (lane + 32 < b) a1 = cfma(ld2(u + lane + 32), xc, a1);
+            u0[i] = (col < c1 && lane < b) ? ld2(u + lane) : mk(0.0, 0.0);
+            u1[i] = (col < c1 && lane + 32 < b) ? ld2(u + lane + 32) : mk(0.0, 0.0);
+        }
+        if (!wait_panel(flags, c, epoch, status, abort_word, ok)) break;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int col = c0 + wp + 8 * i;
+            const cd xc = (col < c1) ? ldcg2(x + col) : mk(0.0, 0.0);
+            a0 = cfma(u0[i], xc, a0);
+            a1 = cfma(u1[i], xc, a1);
         }
     }
     red[wp * LDL_NB + lane] = make_double2(a0.x, a0.y);

@@ -9,12 +9,16 @@
 // The factorisation is right-looking over 64-row panels and runs entirely
 // in the upper triangle, which holds the working Schur complement W(r,c),
 // r < c; the working diagonal lives in dw.  Per panel p = [p0,p1):
-//   k_ldl_diag    eliminate the 64 x 64 diagonal block in shared memory,
+//   k_ldl_diag    eliminate the 64 x 64 diagonal block in registers,
 //                 producing U (= L^H) and invD;
 //   k_ldl_trsm    Wun(p, c) by substitution with U_pp, U(p, c) = invD Wun;
 //   k_ldl_bulk    W(r, c) -= sum_q conj(U(q,r)) Wun(q,c), r <= c beyond p
-//                 (the Hermitian rank-64 trailing update, a complex GEMM);
+//                 (the Hermitian trailing update, a complex GEMM);
 //   k_ldl_linv    after the last panel: (U_pp^H)^-1 of every new panel.
+// Panels are taken in pairs: the second panel's rows are updated by the
+// first (rank 64) before it is eliminated, and the rest of the matrix by
+// both at once (rank 128), which halves the passes over the trailing
+// triangle and doubles the inner dimension of its products.
 // The off-diagonal recurrence and the pivot d = conj(.) follow
 // src/linalg.f90:359-391 term for term; only the summation order differs,
 // and the pivots are kept real (the reference's complex arithmetic leaves a
@@ -61,22 +65,6 @@ __global__ void __launch_bounds__(256) k_ldl_mirror(cd* __restrict__ A, int ld, 
     }
 }
 
-// Diagonal block elimination, blocked by 8-row sub-panels.  The working
-// 64 x 64 upper triangle W(r, c), r <= c (diagonal from dw), sits in shared
-// memory.  Per sub-panel (rows s0..s0+7):
-//   (a) one thread eliminates the 8 x 8 diagonal sub-block in its
-//       registers;
-//   (b) one thread per column c beyond the sub-block forms the unscaled
-//       rows Wun(q, c) = W(q, c) - sum_{q' < q} conj(U(q', q)) Wun(q', c)
-//       by substitution and U(q, c) = invD_q Wun(q, c);
-//   (c) the eight warps apply the rank-8 update W(r, c) -= sum_q
-//       conj(U(q, r)) Wun(q, c) to the rows and columns beyond the
-//       sub-panel on the FP64 tensor cores.
-// Three barriers per sub-panel.  The recurrence and the pivot
-// d = conj(W(q, q)) follow src/linalg.f90:359-391; pivots are real (the
-// imaginary part of W(q, q) is rounding noise of the updates and is
-// dropped: kept, it sets a floor of 1e-13..1e-12 under GHEPIIS's residual
-// NormOfDiff).
 // one m8n8k4 FP64 tensor-core product, D = A B + C (C = D in place)
 __device__ __forceinline__ void mma_f64(double& c0, double& c1, double a, double b)
 {
@@ -86,155 +74,89 @@ __device__ __forceinline__ void mma_f64(double& c0, double& c1, double a, double
 }
 
 constexpr int DG_LD = LDL_NB + 1;
-constexpr int DG_SUB = 8;
-constexpr size_t DG_SMEM = (size_t)(LDL_NB * DG_LD + DG_SUB * LDL_NB) * sizeof(double2);
 
+// Diagonal block elimination: the working 64 x 64 upper triangle W(r, c),
+// r <= c (diagonal from dw), is held in registers, element (r, c) by lane
+// r mod 32 of warp c mod 8 (two rows and eight columns per thread, so the
+// loads and stores of a warp are whole column segments).  Per pivot q the
+// eight threads holding row q publish it to shared memory; after one
+// barrier every thread reads the pivot d = W(q, q) (real: the imaginary
+// part of W(q, q) is rounding noise of the updates; kept, it sets a floor
+// of 1e-13..1e-12 under GHEPIIS's residual NormOfDiff), and applies the
+// rank-one update W(r, c) -= conj(U(q, r)) Wun(q, c), U(q, r) = Wun(q, r)/d,
+// to its elements with q < r <= c; the row-q holders scale their row to
+// U(q, c).  Column groups beyond q are tested per warp, the rows below 32
+// per block, so finished parts cost no issue slots.  The recurrence and
+// the pivot d = conj(W(q, q)) follow src/linalg.f90:359-391; only the
+// summation order differs from the reference's row-by-row dot products.
 __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, int p0, int p1, cd* __restrict__ dw,
                                                    cd* __restrict__ invD, int* __restrict__ status)
 {
-    extern __shared__ double2 dsm[];
-    double2* Ws = dsm;                   // Ws[r * DG_LD + c], r <= c
-    double2* Wu = dsm + LDL_NB * DG_LD;  // Wu[q * LDL_NB + c]: unscaled rows of the sub-panel
-    __shared__ double sid[DG_SUB];       // invD of the sub-panel rows
+    __shared__ double2 rb[2][LDL_NB];
     const int b = p1 - p0;
-    const int tid = threadIdx.x;
-    for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
-        const int r = e & 63, c = e >> 6;
-        double2 v = make_double2(0.0, 0.0);
-        if (r < b && c < b) {
-            if (r < c) {
-                const cd a = A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld];
-                v = make_double2(a.x, a.y);
-            } else if (r == c) {
-                const cd a = dw[p0 + r];
-                v = make_double2(a.x, a.y);
-            }
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    double wr[2][8], wi[2][8];
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+        for (int a = 0; a < 8; a++) {
+            const int r = lane + 32 * j, c = wp + 8 * a;
+            cd v = cd{0.0, 0.0};
+            if (c < b && r <= c) v = (r == c) ? dw[p0 + r] : A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld];
+            wr[j][a] = v.x;
+            wi[j][a] = v.y;
         }
-        Ws[r * DG_LD + c] = v;
-    }
-    __syncthreads();
-    for (int s0 = 0; s0 < b; s0 += DG_SUB) {
-        const int nq = min(DG_SUB, b - s0);
-        // (a) 8 x 8 diagonal sub-block, in the registers of one thread: no
-        // shuffles, so a pivot step costs one reciprocal and three dependent
-        // FP64 operations
-        if (tid == 0) {
-            cd a[DG_SUB][DG_SUB];
+    for (int q = 0; q < b; q++) {
+        const int buf = q & 1, jq = q >> 5;
+        if (lane == (q & 31)) {
 #pragma unroll
-            for (int i = 0; i < DG_SUB; i++)
+            for (int j = 0; j < 2; j++)
+                if (j == jq) {
 #pragma unroll
-                for (int j = i; j < DG_SUB; j++) {
-                    const double2 v = (j < nq) ? Ws[(s0 + i) * DG_LD + s0 + j] : make_double2(0.0, 0.0);
-                    a[i][j] = cd{v.x, v.y};
+                    for (int a = 0; a < 8; a++) rb[buf][wp + 8 * a] = make_double2(wr[j][a], wi[j][a]);
                 }
-#pragma unroll
-            for (int q = 0; q < DG_SUB; q++) {
-                if (q < nq) {
-                    const double dr = a[q][q].x;  // pivot d = conj(W(q,q)), real
-                    const double id = (dr != 0.0) ? __drcp_rn(dr) : 0.0;
-                    sid[q] = id;
-                    invD[p0 + s0 + q] = cd{id, 0.0};
-                    if (dr == 0.0) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + s0 + q + 1);
-                    cd u[DG_SUB];
-#pragma unroll
-                    for (int j = q + 1; j < DG_SUB; j++) u[j] = cd{a[q][j].x * id, a[q][j].y * id};  // U(q, j)
-#pragma unroll
-                    for (int i = q + 1; i < DG_SUB; i++)
-#pragma unroll
-                        for (int j = i; j < DG_SUB; j++) a[i][j] = cfms(conj(u[i]), a[q][j], a[i][j]);
-#pragma unroll
-                    for (int j = q + 1; j < DG_SUB; j++) a[q][j] = u[j];
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < DG_SUB; i++)
-#pragma unroll
-                for (int j = i + 1; j < DG_SUB; j++)
-                    if (j < nq) Ws[(s0 + i) * DG_LD + s0 + j] = make_double2(a[i][j].x, a[i][j].y);
         }
         __syncthreads();
-        // (b) sub-panel rows beyond the sub-block, one thread per column
-        const int t0 = s0 + DG_SUB;
-        if (t0 < b && tid < b - t0) {
-            const int c = t0 + tid;
-            cd wun[DG_SUB];
+        const double d = rb[buf][q].x;
+        const double inv = (d != 0.0) ? __drcp_rn(d) : 0.0;
+        if (threadIdx.x == 0) {
+            invD[p0 + q] = cd{inv, 0.0};
+            if (d == 0.0) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + q + 1);
+        }
+        double ur[2], ui[2];
 #pragma unroll
-            for (int q = 0; q < DG_SUB; q++) {
-                if (q < nq) {
-                    const double2 w = Ws[(s0 + q) * DG_LD + c];
-                    cd v = cd{w.x, w.y};
+        for (int j = 0; j < 2; j++) {
+            const double2 u = rb[buf][lane + 32 * j];  // conj(U(q, r)) = conj(Wun(q, r)) / d
+            ur[j] = u.x * inv;
+            ui[j] = -u.y * inv;
+        }
 #pragma unroll
-                    for (int q2 = 0; q2 < q; q2++) {
-                        const double2 u = Ws[(s0 + q2) * DG_LD + s0 + q];  // U(q2, q)
-                        v = cfms(cd{u.x, -u.y}, wun[q2], v);
+        for (int a = 0; a < 8; a++) {
+            const int c = wp + 8 * a;
+            if (c > q) {  // warp-uniform
+                const double2 v = rb[buf][c];
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int r = lane + 32 * j;
+                    if (j == 0 && q >= 32) continue;  // block-uniform: rows below 32 are finished
+                    if (r > q && r <= c) {
+                        wr[j][a] = fma(-ur[j], v.x, fma(ui[j], v.y, wr[j][a]));
+                        wi[j][a] = fma(-ur[j], v.y, fma(-ui[j], v.x, wi[j][a]));
+                    } else if (r == q) {
+                        wr[j][a] *= inv;
+                        wi[j][a] *= inv;
                     }
-                    wun[q] = v;
-                    Wu[q * LDL_NB + c] = make_double2(v.x, v.y);
-                    const double id = sid[q];
-                    Ws[(s0 + q) * DG_LD + c] = make_double2(v.x * id, v.y * id);
-                } else {
-                    wun[q] = cd{0.0, 0.0};
                 }
             }
         }
-        __syncthreads();
-        // (c) rank-8 update of the rows and columns beyond the sub-panel on
-        // the FP64 tensor cores: 8 x 8 output tiles of the upper triangle
-        // (tile row <= tile column) spread over the eight warps; per tile
-        // and k-step of 4, four m8n8k4 products with the conjugate and the
-        // minus sign folded into the U fragment, accumulated onto W.
-        if (t0 < b) {
-            const int lane = tid & 31, wp = tid >> 5;
-            const int g = lane >> 2, t4 = lane & 3;
-            const int T = (b - t0 + 7) >> 3;
-            const int ntiles = T * (T + 1) / 2;
-            for (int tile = wp; tile < ntiles; tile += 8) {
-                int R = 0, rem = tile;
-                while (rem >= T - R) {
-                    rem -= T - R;
-                    R++;
-                }
-                const int Cc = R + rem;
-                const int r = t0 + 8 * R + g;         // fragment row (C and U)
-                const int cg = t0 + 8 * Cc + g;       // fragment column of Wun
-                const int ca = t0 + 8 * Cc + 2 * t4;  // C columns ca, ca + 1
-                double accr[2], acci[2];
-#pragma unroll
-                for (int e = 0; e < 2; e++) {
-                    const int c = ca + e;
-                    double2 w = make_double2(0.0, 0.0);
-                    if (r < b && c < b && r <= c) w = Ws[r * DG_LD + c];
-                    accr[e] = w.x;
-                    acci[e] = w.y;
-                }
-#pragma unroll
-                for (int k0 = 0; k0 < DG_SUB; k0 += 4) {
-                    const int q = k0 + t4;
-                    double2 u = make_double2(0.0, 0.0), v = make_double2(0.0, 0.0);
-                    if (q < nq && r < b) u = Ws[(s0 + q) * DG_LD + r];  // U(q, r)
-                    if (q < nq && cg < b) v = Wu[q * LDL_NB + cg];      // Wun(q, c)
-                    // W -= conj(U) Wun: Re -= Ur Vr + Ui Vi, Im -= Ur Vi - Ui Vr
-                    mma_f64(accr[0], accr[1], -u.x, v.x);
-                    mma_f64(accr[0], accr[1], -u.y, v.y);
-                    mma_f64(acci[0], acci[1], -u.x, v.y);
-                    mma_f64(acci[0], acci[1], u.y, v.x);
-                }
-#pragma unroll
-                for (int e = 0; e < 2; e++) {
-                    const int c = ca + e;
-                    if (r < b && c < b && r <= c) Ws[r * DG_LD + c] = make_double2(accr[e], acci[e]);
-                }
-            }
-        }
-        __syncthreads();
     }
-    for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
-        const int r = e & 63, c = e >> 6;
-        if (r < c && c < b) {
-            const double2 v = Ws[r * DG_LD + c];
-            A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld] = cd{v.x, v.y};
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+        for (int a = 0; a < 8; a++) {
+            const int r = lane + 32 * j, c = wp + 8 * a;
+            if (c < b && r < c) A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld] = cd{wr[j][a], wi[j][a]};
         }
-    }
 }
 
 // Inverse of the unit lower diagonal block L_pp = U_pp^H of every panel in
@@ -294,10 +216,10 @@ __global__ void __launch_bounds__(256) k_ldl_linv(const cd* __restrict__ A, int 
 //   U(q, c)   = invD_q Wun(q, c);  vbuf(q, c) = Wun(q, c)
 // (the forward form of src/linalg.f90:384-389 for a whole panel).  One warp
 // per column, lanes hold rows lane and lane + 32; U_pp comes from A through
-// shared memory.  32 columns per CTA.
+// shared memory.  vbuf(q, c) sits at vbuf[c * vld + q].
 constexpr int TRSM_COLS = 8;
 __global__ void __launch_bounds__(256) k_ldl_trsm(cd* __restrict__ A, int ld, int p0, int p1, int c0, int n,
-                                                   const cd* __restrict__ invD, cd* __restrict__ vbuf)
+                                                   const cd* __restrict__ invD, cd* __restrict__ vbuf, int vld)
 {
     extern __shared__ double2 sm[];
     double2* U = sm;  // U[q*DG_LD + r] = U(q, r), q < r
@@ -335,7 +257,7 @@ __global__ void __launch_bounds__(256) k_ldl_trsm(cd* __restrict__ A, int ld, in
                 w1 = cfms(cd{uq.x, -uq.y}, wq, w1);
             }
         }
-        cd* v = vbuf + (size_t)c * LDL_NB;
+        cd* v = vbuf + (size_t)c * vld;
         if (r0 < b) {
             v[r0] = w0;
             col[r0] = cmul(w0, d0);
@@ -372,7 +294,8 @@ constexpr size_t blk_smem() { return (size_t)2 * BLK_KC * (BLK_P + blk_vp<TC>())
 
 template <int TC, int WR, int WC>
 __global__ void __launch_bounds__(256, TC == 64 ? 3 : 4) k_ldl_bulk(cd* __restrict__ A, int ld, int p0, int p1, int r0, int rend,
-                                                   int c0, int n, const cd* __restrict__ vbuf, cd* __restrict__ dw)
+                                                   int c0, int n, const cd* __restrict__ vbuf, int vld,
+                                                   cd* __restrict__ dw)
 {
     constexpr int MT = LDL_NB / WR / 8;  // 8 x 8 tiles per warp along rows
     constexpr int NT = TC / WC / 8;      // and along columns
@@ -383,6 +306,13 @@ __global__ void __launch_bounds__(256, TC == 64 ? 3 : 4) k_ldl_bulk(cd* __restri
     if (rb > cb + TC - 1) return;  // tile entirely below the diagonal
     const int b = p1 - p0;
     const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    {
+        // bring the tile's old values towards L2 now; they are read after
+        // the products (64 rows x 16 B = eight 128-byte lines per column)
+        const int cc = cb + (tid >> 3), rr = rb + 8 * (tid & 7);
+        if (cc < n && (tid >> 3) < TC && rr < rend && rr <= cc)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(A + (size_t)rr + (size_t)cc * ld));
+    }
     const int wr = wp / WC, wc = wp % WC;
     const int g = lane >> 2, t4 = lane & 3;
     double accr[MT][NT][2], acci[MT][NT][2];
@@ -408,7 +338,7 @@ __global__ void __launch_bounds__(256, TC == 64 ? 3 : 4) k_ldl_bulk(cd* __restri
             const int c = cb + mm;
             const bool kv = (k0 + q < b) && (c < n);
             cp_async16(Vs + q * VP + mm,
-                       kv ? (const void*)(vbuf + (size_t)(k0 + q) + (size_t)c * LDL_NB) : (const void*)vbuf, kv ? 16 : 0);
+                       kv ? (const void*)(vbuf + (size_t)(k0 + q) + (size_t)c * vld) : (const void*)vbuf, kv ? 16 : 0);
         }
         cp_async_commit();
     };
@@ -467,18 +397,19 @@ static bool g_ldl_attr = false;
 
 // Trailing update by panel [p0, p1) of rows [r0, rend), columns
 // [max(r, c0), n).
-static void launch_update(Ctx& c, cudaStream_t st, const cd* vb, int p0, int p1, int r0, int rend, int c0, int n)
+// k rows [p0, p1) of U and of vb (vb(q, c) at vb[c * vld + q - p0]).
+static void launch_update(Ctx& c, cudaStream_t st, const cd* vb, int vld, int p0, int p1, int r0, int rend, int c0,
+                          int n)
 {
-    if (rend <= r0 || c0 >= n) return;
+    if (rend <= r0 || c0 >= n || p1 <= p0) return;
     const int nrb = (rend - r0 + LDL_NB - 1) / LDL_NB;
     if (nrb == 1) {
-        // one panel of rows (the lookahead rows): narrow 64 x 16 tiles so
-        // that enough CTAs run
+        // one panel of rows: narrow 64 x 16 tiles so that enough CTAs run
         dim3 g((n - c0 + 15) / 16, 1);
-        k_ldl_bulk<16, 8, 1><<<g, 256, blk_smem<16>(), st>>>(c.F, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
+        k_ldl_bulk<16, 8, 1><<<g, 256, blk_smem<16>(), st>>>(c.F, c.ld, p0, p1, r0, rend, c0, n, vb, vld, c.dw);
     } else {
         dim3 g((n - c0 + 31) / 32, nrb);
-        k_ldl_bulk<32, 4, 2><<<g, 256, blk_smem<32>(), st>>>(c.F, c.ld, p0, p1, r0, rend, c0, n, vb, c.dw);
+        k_ldl_bulk<32, 4, 2><<<g, 256, blk_smem<32>(), st>>>(c.F, c.ld, p0, p1, r0, rend, c0, n, vb, vld, c.dw);
     }
     c.launches++;
 }
@@ -489,6 +420,16 @@ static void enqueue_factor(Ctx& c, int m0, int n, const std::vector<int>& starts
     const size_t sm1 = LDL_NB * DG_LD * sizeof(double2);
     const int nblk = (int)starts.size();
     auto blk_end = [&](int i) { return (i + 1 < nblk) ? starts[i + 1] : n; };
+    auto trsm = [&](int p0, int p1, int cfrom, cd* vb) {
+        if (cfrom >= n) return;
+        k_ldl_trsm<<<(n - cfrom + TRSM_COLS - 1) / TRSM_COLS, 256, sm1, c.stream>>>(c.F, c.ld, p0, p1, cfrom, n,
+                                                                                   c.invD, vb, LDL_VLD);
+        c.launches++;
+    };
+    auto diag = [&](int p0, int p1) {
+        k_ldl_diag<<<1, 256, 0, c.stream>>>(c.F, c.ld, p0, p1, c.dw, c.invD, c.status);
+        c.launches++;
+    };
     if (n > m0) {
         const int ct0 = m0 / 32, ct1 = (n + 31) / 32;
         dim3 g(ct1 - ct0, ct1);
@@ -499,39 +440,49 @@ static void enqueue_factor(Ctx& c, int m0, int n, const std::vector<int>& starts
     for (int i = 0; i < nexist; i++) {
         const int p0 = starts[i], p1 = std::min(blk_end(i), m0);
         if (p1 <= p0 || m0 >= n) continue;
-        k_ldl_trsm<<<(n - m0 + TRSM_COLS - 1) / TRSM_COLS, 256, sm1, c.stream>>>(c.F, c.ld, p0, p1, m0, n, c.invD,
-                                                                                c.vbuf);
-        c.launches++;
-        launch_update(c, c.stream, c.vbuf, p0, p1, p1, n, m0, n);
+        trsm(p0, p1, m0, c.vbuf);
+        launch_update(c, c.stream, c.vbuf, LDL_VLD, p0, p1, p1, n, m0, n);
     }
-    // new panels, right-looking with a lookahead: the rows of the next panel
-    // are updated first on the main stream, so that panel's factorisation
-    // overlaps the trailing update running on the side stream.  The
-    // trailing update of panel i is split: first the rows of panel i+2
-    // (after which lev[1] is recorded; the lookahead update of panel i+1
-    // needs only those), then the rest, which thus has two panel steps to
-    // complete before the lookahead of panel i+2 touches its rows.  Three
-    // panel buffers rotate, so a buffer is rewritten only after the update
-    // that reads it has finished (stream order through lev[1]).
+    // new panels in pairs (A = [a0, a1), B = [a1, b1), B may be empty),
+    // right-looking with a lookahead: per pair,
+    //   main stream: A's diagonal block and rows; B's rows updated by A
+    //     (rank 64); B's diagonal block and rows; then the rows of the next
+    //     pair updated by this one (rank 128), so the next pair's
+    //     factorisation can start while
+    //   the side stream updates the rest (rank 128): first the rows of the
+    //     pair after next (after which lev[1] is recorded; the next pair's
+    //     lookahead update needs only those), then everything beyond, which
+    //     thus has two pair steps to complete before the lookahead of the
+    //     pair after next touches its rows.
+    // Three buffers of unscaled rows rotate, so a buffer is rewritten only
+    // after the updates that read it have finished (stream order through
+    // lev[1]).
     bool bulk_recorded = false;  // lev[1] recorded by this sequence (never wait on an older record)
-    for (int i = nexist; i < nblk; i++) {
-        const int p0 = starts[i], p1 = blk_end(i);
-        const int p2 = (i + 1 < nblk) ? blk_end(i + 1) : n;
-        const int p3 = (i + 2 < nblk) ? blk_end(i + 2) : n;
-        cd* vb = c.vbuf + (size_t)((i - nexist) % 3) * LDL_NB * c.ld;
-        k_ldl_diag<<<1, 256, DG_SMEM, c.stream>>>(c.F, c.ld, p0, p1, c.dw, c.invD, c.status);
-        c.launches++;
-        if (p1 >= n) break;
-        k_ldl_trsm<<<(n - p1 + TRSM_COLS - 1) / TRSM_COLS, 256, sm1, c.stream>>>(c.F, c.ld, p0, p1, p1, n, c.invD, vb);
-        c.launches++;
+    int step = 0;
+    for (int i = nexist; i < nblk; i += 2, step++) {
+        const int a0 = starts[i], a1 = blk_end(i);
+        const bool hasB = i + 1 < nblk;
+        const int b1 = hasB ? blk_end(i + 1) : a1;
+        const int n1 = (i + 3 < nblk) ? blk_end(i + 3) : n;  // end of the next pair
+        const int n2 = (i + 5 < nblk) ? blk_end(i + 5) : n;  // end of the pair after next
+        cd* vb = c.vbuf + (size_t)(step % 3) * LDL_VLD * c.ld;
+        diag(a0, a1);
+        if (a1 >= n) break;
+        trsm(a0, a1, a1, vb);
+        if (hasB) {
+            launch_update(c, c.stream, vb, LDL_VLD, a0, a1, a1, b1, a1, n);
+            diag(a1, b1);
+            if (b1 >= n) break;
+            trsm(a1, b1, b1, vb + LDL_NB);
+        }
         cudaEventRecord(c.lev[0], c.stream);
-        // rows of the next panel wait for the previous trailing update's first part
+        // rows of the next pair wait for the previous pair's first part
         if (bulk_recorded) cudaStreamWaitEvent(c.stream, c.lev[1], 0);
-        launch_update(c, c.stream, vb, p0, p1, p1, p2, p1, n);
+        launch_update(c, c.stream, vb, LDL_VLD, a0, b1, b1, n1, b1, n);
         cudaStreamWaitEvent(c.side, c.lev[0], 0);
-        launch_update(c, c.side, vb, p0, p1, p2, p3, p2, n);
+        launch_update(c, c.side, vb, LDL_VLD, a0, b1, n1, n2, n1, n);
         cudaEventRecord(c.lev[1], c.side);
-        launch_update(c, c.side, vb, p0, p1, p3, n, p3, n);
+        launch_update(c, c.side, vb, LDL_VLD, a0, b1, n2, n, n2, n);
         bulk_recorded = true;
     }
     if (bulk_recorded) {
@@ -556,7 +507,6 @@ int ldlh_factor(Ctx& c, int m0, int n)
     const size_t sm1 = LDL_NB * DG_LD * sizeof(double2);
     if (!g_ldl_attr) {
         cudaFuncSetAttribute(k_ldl_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
-        cudaFuncSetAttribute(k_ldl_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DG_SMEM);
         cudaFuncSetAttribute(k_ldl_linv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * sm1));
         cudaFuncSetAttribute(k_ldl_bulk<32, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem<32>());
         cudaFuncSetAttribute(k_ldl_bulk<16, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem<16>());

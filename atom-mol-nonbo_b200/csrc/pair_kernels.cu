@@ -513,6 +513,38 @@ __global__ void __launch_bounds__(256) k_adjoint(SysParams sp, const double* __r
     }
 }
 
+// dE/d(vech L, vech B) of one function from its summed adjoint values v
+// (NP complex sums of w Z, then the sum of Re(w a)) and its parameters p;
+// lane x < NP writes entry x of both halves of g.
+template <int N>
+__device__ __forceinline__ void adj_gradient(const double (&v)[AdjNV<N>::value], const double* __restrict__ p,
+                                             int lane, double* __restrict__ g)
+{
+    constexpr int NP = Sym<N>::NP;
+    constexpr int NV = AdjNV<N>::value;
+    if (lane < NP) {
+        // vech entry x = (column i, row j >= i)
+        int i = 0, x = lane;
+        while (x >= N - i) {
+            x -= N - i;
+            i++;
+        }
+        const int j = i + x;
+        double acc = 0.0;
+        for (int m = i; m < N; m++) {
+            // A(j,m) from the packed lower triangle, L(m,i) = vech(i,m)
+            const int a = (j >= m) ? vech_index(N, m, j) : vech_index(N, j, m);
+            acc += v[2 * a] * p[vech_index(N, i, m)];
+        }
+        double gL = -4.0 * acc;
+        if (i == j) gL += 2.0 * v[NV - 1] / p[vech_index(N, i, i)];
+        const int a = vech_index(N, i, j);
+        const double gB = -2.0 * ((i == j) ? 1.0 : 2.0) * v[2 * a + 1];
+        g[lane] = gL;
+        g[NP + lane] = gB;
+    }
+}
+
 // One warp per function f in [nfru, nfa): sum its row and column partials
 // in a fixed order and form dE/d(vech L_f, vech B_f).
 template <int N>
@@ -546,29 +578,7 @@ __global__ void __launch_bounds__(256) k_adjoint_final(const double* __restrict_
     for (int s = 16; s >= 1; s >>= 1)
 #pragma unroll
         for (int x = 0; x < NV; x++) v[x] += __shfl_xor_sync(0xffffffffu, v[x], s);
-    if (lane < NP) {
-        // vech entry x = (column i, row j >= i)
-        int i = 0, x = lane;
-        while (x >= N - i) {
-            x -= N - i;
-            i++;
-        }
-        const int j = i + x;
-        const double* p = params + (size_t)f * 2 * NP;
-        double acc = 0.0;
-        for (int m = i; m < N; m++) {
-            // A(j,m) from the packed lower triangle, L(m,i) = vech(i,m)
-            const int a = (j >= m) ? vech_index(N, m, j) : vech_index(N, j, m);
-            acc += v[2 * a] * p[vech_index(N, i, m)];
-        }
-        double gL = -4.0 * acc;
-        if (i == j) gL += 2.0 * v[NV - 1] / p[vech_index(N, i, i)];
-        const int a = vech_index(N, i, j);
-        const double gB = -2.0 * ((i == j) ? 1.0 : 2.0) * v[2 * a + 1];
-        double* g = grad + (size_t)(f - nfru) * 2 * NP;
-        g[lane] = gL;
-        g[NP + lane] = gB;
-    }
+    adj_gradient<N>(v, params + (size_t)f * 2 * NP, lane, grad + (size_t)(f - nfru) * 2 * NP);
 }
 
 // Contraction of Glob_D, src/workproc.f90:2127-2142: one CTA per function.
@@ -724,6 +734,117 @@ __global__ void __launch_bounds__(W * 32) k_cand_row(SysParams sp, const double*
         stcd(Scol + o, conj(s));
         stcd(Mcol + o, conj(m));
     }
+}
+
+// Gradient of every candidate's energy with respect to its own parameters:
+// what EnergyIB(nbase, nbase+1) (src/workproc.f90:2063-2154, nfo = 1) returns
+// once candidate j is function K = nbase+1 and its eigenpair is (E_j, c),
+// c = x / sqrt(x^H S x) (SpecifNorm 0).  Only the pairs (K, q), q <= nbase,
+// hold derivatives with respect to function K; each is recomputed with the
+// bra derivative contracted (term_adjoint) and weighted w = conj(c_K) c_q
+// f_Kq, q = nbase being the diagonal pair (the candidate with itself).
+// CTA (chunk, j): 128 threads over q, summed in a fixed order (butterflies,
+// then warps in order) into part[(j * nchunk + chunk) * NV].
+constexpr int CAND_ADJ_NT = 128;
+
+template <int N>
+__global__ void __launch_bounds__(CAND_ADJ_NT) k_cand_adjoint(
+    SysParams sp, const double* __restrict__ coef, const double* __restrict__ Pd, const cd* __restrict__ cbra,
+    const cd* __restrict__ cket, const double* __restrict__ cdet, const double* __restrict__ cdS,
+    const cd* __restrict__ ket, const double* __restrict__ detL, const double* __restrict__ diagS, int nbase,
+    const cd* __restrict__ V, int ldv, const cd* __restrict__ vK, const double* __restrict__ t1,
+    const double* __restrict__ energy, const int* __restrict__ err, double* __restrict__ part)
+{
+    constexpr int NP = Sym<N>::NP;
+    constexpr int NV = AdjNV<N>::value;
+    __shared__ double red[CAND_ADJ_NT / 32][NV];
+    const int j = blockIdx.y;
+    const int q = blockIdx.x * CAND_ADJ_NT + threadIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double v[NV];
+#pragma unroll
+    for (int x = 0; x < NV; x++) v[x] = 0.0;
+    if (q <= nbase && err[j] != 1) {
+        const double rs = 1.0 / sqrt(t1[j]);
+        const double E = energy[j];
+        const cd cK = rs * vK[j];
+        const bool dg = (q == nbase);
+        cd Ck[N][N];
+        load_sym<N>(cbra + (size_t)j * NP, Ck);
+        const cd* kq = dg ? cket + (size_t)j * sp.T * NP : ket + (size_t)q * sp.T * NP;
+        const double dq = dg ? cdet[j] : detL[q];
+        const double dSq = dg ? cdS[j] : diagS[q];
+        const cd cq = dg ? cK : rs * ldcd(V + (size_t)j * ldv + q);
+        const double absdet = fabs(dq * cdet[j]);
+        cd Zk[NP], Zl[NP], a = mk(0.0, 0.0);
+#pragma unroll
+        for (int x = 0; x < NP; x++) Zk[x] = mk(0.0, 0.0);
+#pragma unroll 1
+        for (int t = 0; t < sp.T; t++) {
+            cd tCl[N][N];
+            load_sym<N>(kq + (size_t)t * NP, tCl);
+            TermEnergy<N> te;
+            term_energy<N, true>(Ck, tCl, absdet, sp, te);
+            double P[N][N];
+            load_P<N>(Pd, t, P);
+            term_adjoint<N, false>(P, Ck, tCl, te, sp, E, __ldg(coef + t), Zk, Zl, a);
+        }
+        const cd wq = (1.0 / sqrt(cdS[j] * dSq)) * cmul(conj(cK), cq);
+#pragma unroll
+        for (int x = 0; x < NP; x++) {
+            const cd z = cmul(wq, Zk[x]);
+            v[2 * x] = z.x;
+            v[2 * x + 1] = z.y;
+        }
+        v[NV - 1] = cmul(wq, a).x;
+    }
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1)
+#pragma unroll
+        for (int x = 0; x < NV; x++) v[x] += __shfl_xor_sync(0xffffffffu, v[x], s);
+    if (lane == 0)
+#pragma unroll
+        for (int x = 0; x < NV; x++) red[w][x] = v[x];
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double s = 0.0;
+#pragma unroll
+        for (int u = 0; u < CAND_ADJ_NT / 32; u++) s += red[u][threadIdx.x];
+        part[((size_t)j * gridDim.x + blockIdx.x) * NV + threadIdx.x] = s;
+    }
+}
+
+// One warp per candidate: the chunk sums in order, then the gradient
+// (NaN where the candidate's factorisation hit a zero pivot).
+template <int N>
+__global__ void __launch_bounds__(256) k_cand_adjoint_final(const double* __restrict__ part, int nchunk,
+                                                            const double* __restrict__ cpar,
+                                                            const int* __restrict__ err, int count,
+                                                            double* __restrict__ grad)
+{
+    constexpr int NP = Sym<N>::NP;
+    constexpr int NV = AdjNV<N>::value;
+    const int lane = threadIdx.x & 31;
+    const int j = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    if (j >= count) return;
+    double v[NV];
+#pragma unroll
+    for (int x = 0; x < NV; x++) v[x] = 0.0;
+    for (int u = lane; u < nchunk; u += 32) {
+        const double* src = part + ((size_t)j * nchunk + u) * NV;
+#pragma unroll
+        for (int x = 0; x < NV; x++) v[x] += src[x];
+    }
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1)
+#pragma unroll
+        for (int x = 0; x < NV; x++) v[x] += __shfl_xor_sync(0xffffffffu, v[x], s);
+    double* g = grad + (size_t)j * 2 * NP;
+    if (err[j] == 1) {
+        if (lane < 2 * NP) g[lane] = __longlong_as_double(0x7ff8000000000000LL);
+        return;
+    }
+    adj_gradient<N>(v, cpar + (size_t)j * 2 * NP, lane, g);
 }
 
 // ---------------------------------------------------------------------------
@@ -1041,6 +1162,27 @@ static int cand_rows_n(Ctx& c, CandWork& cw, int nbase, int count, double approx
 int launch_cand_rows(Ctx& c, CandWork& cw, int nbase, int count, double approx_e, int variant)
 {
     ECG_DISPATCH_N(c.n, cand_rows_n, c, cw, nbase, count, approx_e, variant)
+}
+
+template <int N>
+static int cand_adjoint_n(Ctx& c, CandWork& cw, int nbase, int count, const cd* vK, const double* t1,
+                          const double* energy, const int* err, double* grad)
+{
+    constexpr int NV = AdjNV<N>::value;
+    const int nchunk = nbase / CAND_ADJ_NT + 1;  // q = 0..nbase
+    if ((size_t)nchunk * count * NV > cw.gpart_n) return -1;
+    k_cand_adjoint<N><<<dim3(nchunk, count), CAND_ADJ_NT, 0, c.stream>>>(c.sp, c.coef, c.Pd, cw.bra, cw.ket, cw.det,
+                                                                         cw.dS, c.ket, c.detL, c.diagS, nbase, cw.V,
+                                                                         cw.ldv, vK, t1, energy, err, cw.gpart);
+    k_cand_adjoint_final<N><<<(count * 32 + 255) / 256, 256, 0, c.stream>>>(cw.gpart, nchunk, cw.par, err, count,
+                                                                           grad);
+    c.launches += 2;
+    return last_err();
+}
+int launch_cand_adjoint(Ctx& c, CandWork& cw, int nbase, int count, const cd* vK, const double* t1,
+                        const double* energy, const int* err, double* grad)
+{
+    ECG_DISPATCH_N(c.n, cand_adjoint_n, c, cw, nbase, count, vK, t1, energy, err, grad)
 }
 
 }  // namespace ecg

@@ -30,6 +30,8 @@ PROTOTYPES = {
                                         _dp, _ip]),
     "ecg_eval_candidates": (C.c_int, [_vp, C.c_int, C.c_int, _dp, C.c_double, C.c_double, C.c_int, _dp, _ip, _ip,
                                       _dp]),
+    "ecg_eval_candidates_grad": (C.c_int, [_vp, C.c_int, C.c_int, _dp, C.c_double, C.c_double, C.c_int, _dp, _ip,
+                                           _ip, _dp, _dp]),
     "ecg_energy_ga": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _ip]),
     "ecg_energy_gb": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]),
     "ecg_energy_gb_adjoint": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]),

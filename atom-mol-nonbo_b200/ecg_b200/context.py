@@ -300,6 +300,24 @@ class Context:
                "ecg_eval_candidates")
         return E, err, it, ra
 
+    def eval_candidates_grad(self, nbase, candidates, approx_energy, tol, max_iter=20):
+        """eval_candidates plus, per candidate, the gradient EnergyIB(nbase,
+        nbase+1) (src/workproc.f90:2063-2154) returns for it as function
+        nbase+1.  Returns (E, ErrorCode, NumIter, RelAcc, grad (count, npt))."""
+        cand = np.ascontiguousarray(candidates, dtype=np.float64)
+        if cand.ndim != 2 or cand.shape[1] != self.npt:
+            raise ValueError(f"candidates must be (count, {self.npt})")
+        cnt = cand.shape[0]
+        E = np.zeros(cnt)
+        err = np.zeros(cnt, dtype=np.int32)
+        it = np.zeros(cnt, dtype=np.int32)
+        ra = np.zeros(cnt)
+        g = np.zeros((cnt, self.npt))
+        _check(self.lib.ecg_eval_candidates_grad(self.h, int(nbase), cnt, dptr(cand), float(approx_energy),
+                                                 float(tol), int(max_iter), dptr(E), iptr(err), iptr(it), dptr(ra),
+                                                 dptr(g)), "ecg_eval_candidates_grad")
+        return E, err, it, ra, g
+
     def matrix_elements(self, pk, pl, terms, gradflag=0):
         """MatrixElements for a batch: returns H, S (count,) and Dk, Dl
         (count, 4np) complex (None when not requested)."""

@@ -128,6 +128,22 @@ int ecg_eval_candidates(ecg_ctx* ctx, int nbase, int count, const double* cand_h
                         double tol, int max_iter, double* energies_host, int* errcodes_host, int* num_iter_host,
                         double* rel_acc_host);
 
+/* ecg_eval_candidates plus, for every candidate j, the gradient that
+ *     Glob_NonlinParam(1:npt, nbase+1) = cand_host(1:npt, j)
+ *     call EnergyIB(E_j, grad_j, .true., ErrorCode_j)   with nfru = nbase,
+ *                                                        nfa = nbase+1
+ * returns (src/workproc.f90:2063-2154 with nfo = 1): dE_j / d(vech L,
+ * vech B) of the candidate itself, from its eigenpair normalised c^H S c = 1
+ * and a fused adjoint pass over row nbase+1 (no Glob_D).  This is the
+ * energy + gradient the optimisation of a newly added function needs
+ * (BasisEnlI's DRMNG loop, src/workproc.f90:4137-4170, and OptCycleI),
+ * for all candidates at once.  grad_host receives npt x count values
+ * (NaN for a candidate whose ErrorCode is 1); requires nbase >= 1.  Other
+ * arguments and outputs as for ecg_eval_candidates. */
+int ecg_eval_candidates_grad(ecg_ctx* ctx, int nbase, int count, const double* cand_host, double approx_energy,
+                             double tol, int max_iter, double* energies_host, int* errcodes_host, int* num_iter_host,
+                             double* rel_acc_host, double* grad_host);
+
 /* EnergyGA (want_vector 0) / EnergyGAM (want_vector 1), src/workproc.f90:
  * 1697-1838, for contexts created with method 'G': optional
  * ComputeMatElem(Nmin,Nmax), then the which-th smallest eigenvalue of
