@@ -198,10 +198,10 @@ __global__ void __launch_bounds__(256) k_zgemm(const cd* __restrict__ A, int lda
 // so that every item depends only on items with smaller indices, and each
 // CTA takes items blockIdx.x, blockIdx.x + gridDim.x, ... in order, so with
 // all CTAs co-resident every wait ends.  Each wait is bounded
-// (CAND_SPIN_LIMIT polls, or at once after any CTA gave up); a CTA that gives
+// (abort_word[1] polls, SOLVE_SPIN_LIMIT by default, or at once after any
+// CTA gave up); a CTA that gives
 // up records ST_SOLVE_TIMEOUT and publishes nothing.
 // ---------------------------------------------------------------------------
-constexpr int CAND_SPIN_LIMIT = 1 << 22;
 constexpr int TS_LDA = 64 + 2;
 constexpr int TS_LDB = 64 + 4;
 constexpr size_t TS_SMEM = (size_t)(64 * TS_LDA + CAND_NC * TS_LDB) * sizeof(double2);
@@ -346,8 +346,9 @@ __global__ void __launch_bounds__(256) k_cand_solve(const cd* __restrict__ Gm, i
             if (tid == 0) {
                 int gg = 1;
                 int spins = 0;
+                const int limit = ((volatile int*)abort_word)[1];
                 while (ld_acquire_u32(flags + q * ncb + cb) != 1u) {
-                    if (++spins > CAND_SPIN_LIMIT || *((volatile int*)abort_word) != 0) {
+                    if (++spins > limit || *((volatile int*)abort_word) != 0) {
                         gg = 0;
                         break;
                     }
@@ -744,7 +745,7 @@ int ensure_work(Ctx& c, int count)
     r |= dalloc_n(&cw.Pk, (size_t)CAND_KSPLIT * ldv * 2 * CAND_PAD);
     r |= dalloc_n(&cw.flags, (size_t)cw.nflags);
     r |= dalloc_n(&cw.bstart, (size_t)maxpanels + 1);
-    r |= dalloc_n(&cw.abort_word, 1);
+    r |= dalloc_n(&cw.abort_word, 2);  // abort word, wait poll limit
     cw.gpart_n = (size_t)bcap * (c.ld / 128 + 2) * (2 * c.np + 1);
     r |= dalloc_n(&cw.gpart, cw.gpart_n);
     r |= dalloc_n(&cw.grad, (size_t)c.npt * bcap);
@@ -767,6 +768,10 @@ int ensure_work(Ctx& c, int count)
     for (void* p : zc)
         if (cudaMemsetAsync(p, 0, col * sizeof(cd), c.stream) != cudaSuccess) return -2;
     if (cudaMemsetAsync(cw.brd, 0, 4 * (size_t)ccap * sizeof(cd), c.stream) != cudaSuccess) return -2;
+    if (cudaMemcpyAsync(cw.abort_word + 1, &c.wait_limit, sizeof(int), cudaMemcpyHostToDevice, c.stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(c.stream) != cudaSuccess)
+        return -2;
     return 0;
 }
 

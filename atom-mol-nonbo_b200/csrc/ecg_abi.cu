@@ -531,6 +531,7 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
               cudaMemset(c.H, 0, L * L * sizeof(cd)) == cudaSuccess &&
               cudaMemset(c.S, 0, L * L * sizeof(cd)) == cudaSuccess &&
               cudaMemset(c.counters, 0, 4 * sizeof(int)) == cudaSuccess &&
+              cudaMemcpy(c.counters + 3, &c.wait_limit, sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMemset(c.flags, 0, (L + 2) * sizeof(unsigned)) == cudaSuccess &&
               cudaMemset(c.status, 0, ST_COUNT * sizeof(int)) == cudaSuccess &&
               cudaMemset(c.c, 0, L * sizeof(cd)) == cudaSuccess && cudaMemset(c.x, 0, L * sizeof(cd)) == cudaSuccess;
@@ -570,6 +571,18 @@ int ecg_set_params_device(ecg_ctx* ctx, const double* params_dev, int first, int
     Ctx& c = ctx->c;
     CK(cudaMemcpyAsync(c.params + (size_t)(first - 1) * c.npt, params_dev, (size_t)count * c.npt * sizeof(double),
                        cudaMemcpyDeviceToDevice, c.stream));
+    return ECG_OK;
+}
+
+int ecg_set_wait_limit(ecg_ctx* ctx, int polls)
+{
+    if (!ctx) return ECG_EARG;
+    Ctx& c = ctx->c;
+    c.wait_limit = polls < 0 ? SOLVE_SPIN_LIMIT : polls;
+    CK(cudaMemcpyAsync(c.counters + 3, &c.wait_limit, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    if (c.cand.abort_word)
+        CK(cudaMemcpyAsync(c.cand.abort_word + 1, &c.wait_limit, sizeof(int), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
     return ECG_OK;
 }
 

@@ -10,6 +10,11 @@ namespace ecg {
 
 // Pair tiles are 32 x 32 blocks of the lower triangle of the pair matrix.
 constexpr int TILE = 32;
+// Default poll limit of the bounded device waits of the triangular solves
+// (each poll sleeps about 64 ns): a wait that runs out records
+// ST_SOLVE_TIMEOUT and the call reports ECG_ECUDA.
+constexpr int SOLVE_SPIN_LIMIT = 1 << 22;
+
 // LDL^H block size (rows of one panel).
 constexpr int LDL_NB = 64;
 // Trailing updates apply two panels at once (rank 128); the unscaled panel
@@ -135,7 +140,8 @@ struct Ctx {
     int* status_h = nullptr;    // pinned host mirror
     double* red = nullptr;      // reduction scratch for the solver (doubles)
     double* red_h = nullptr;    // pinned host mirror of the reduction results
-    int* counters = nullptr;    // last-block counters for the triangular solves
+    int* counters = nullptr;    // last-block counters [0,1], abort word [2], wait poll limit [3] of the solves
+    int wait_limit = SOLVE_SPIN_LIMIT;
     cd* yv = nullptr;           // forward-solve result (ld)
     cd* zv = nullptr;           // D^-1 scaled forward result (ld)
     cd* spart = nullptr;        // per-CTA partial sums of the blocked solves

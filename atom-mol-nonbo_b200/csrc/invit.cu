@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(256) k_bwd(const cd* __restrict__ A, int ld, i
 // bounded: after SOLVE_SPIN_LIMIT polls, or as soon as any CTA has given
 // up (the abort word), the CTA records ST_SOLVE_TIMEOUT and finishes
 // without waiting; the host then reports the step as failed.
-constexpr int SOLVE_SPIN_LIMIT = 1 << 22;
+static_assert(SOLVE_SPIN_LIMIT == (1 << 22), "the default poll limit of the solves' waits");
 constexpr int LS_LD = LDL_NB + 1;
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
@@ -171,6 +171,8 @@ __device__ __forceinline__ void st_release(unsigned* p, unsigned v)
 }
 
 // Wait (thread 0) for flags[a] == epoch; returns false if this CTA must stop.
+// abort_word[1] holds the poll limit (SOLVE_SPIN_LIMIT unless a caller set
+// another through ecg_set_wait_limit).
 __device__ __forceinline__ bool wait_panel(const unsigned* flags, int a, unsigned epoch, int* status, int* abort_word,
                                            bool& ok)
 {
@@ -179,8 +181,9 @@ __device__ __forceinline__ bool wait_panel(const unsigned* flags, int a, unsigne
         int g = 1;
         if (ok) {
             int spins = 0;
+            const int limit = ((volatile int*)abort_word)[1];
             while (ld_acquire(flags + a) != epoch) {
-                if (++spins > SOLVE_SPIN_LIMIT || *((volatile int*)abort_word) != 0) {
+                if (++spins > limit || *((volatile int*)abort_word) != 0) {
                     g = 0;
                     break;
                 }

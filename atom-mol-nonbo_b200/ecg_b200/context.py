@@ -358,6 +358,10 @@ class Context:
         _check(self.lib.ecg_timer_stop(self.h, C.byref(ms)), "ecg_timer_stop")
         return ms.value
 
+    def set_wait_limit(self, polls):
+        """Poll limit of the solves' bounded device waits (< 0: default)."""
+        _check(self.lib.ecg_set_wait_limit(self.h, int(polls)), "ecg_set_wait_limit")
+
     def io_bytes(self):
         a, b = C.c_longlong(), C.c_longlong()
         _check(self.lib.ecg_io_bytes(self.h, C.byref(a), C.byref(b)), "ecg_io_bytes")

@@ -9,6 +9,7 @@
 !   EnergyIA / EnergyIAM               -> GPU_EnergyIA(Nmin,Nmax,AreMatElemNeeded,SpecifNorm,ErrorCode)
 !   EnergyIB                           -> GPU_EnergyIB(Evalue,Gradient,AreMatElemNeeded,ErrorCode)
 !   BasisEnlI trial loop (Kstep = 1)   -> GPU_EvalTrials(nfru,NTrials,ParSets,Energies,ErrorCodes)
+!   EnergyIB of a new function, batched-> GPU_EvalTrialsGrad(nbase,NTrials,ParSets,Energies,Gradients,ErrorCodes)
 !   EnergyGA / EnergyGAM               -> GPU_EnergyGA(Nmin,Nmax,AreMatElemNeeded,WantVector,ErrorCode)
 !   EnergyGB                           -> GPU_EnergyGB(Evalue,Gradient,AreMatElemNeeded,ErrorCode)
 !   ComputeOverlapPenalty(AndAddGradient) -> GPU_OverlapPenalty(AddGradient,TotalPenalty,Gradient)
@@ -96,6 +97,16 @@ interface
     real(c_double), intent(in) :: cand(*)
     real(c_double), value :: approx_energy, tol
     real(c_double), intent(out) :: energies(*), rel_acc(*)
+    integer(c_int), intent(out) :: errcodes(*), num_iter(*)
+  end function
+  integer(c_int) function ecg_eval_candidates_grad(ctx, nbase, count, cand, approx_energy, tol, max_iter, &
+      energies, errcodes, num_iter, rel_acc, grad) bind(C, name='ecg_eval_candidates_grad')
+    import :: c_int, c_double, c_ptr
+    type(c_ptr), value :: ctx
+    integer(c_int), value :: nbase, count, max_iter
+    real(c_double), intent(in) :: cand(*)
+    real(c_double), value :: approx_energy, tol
+    real(c_double), intent(out) :: energies(*), rel_acc(*), grad(*)
     integer(c_int), intent(out) :: errcodes(*), num_iter(*)
   end function
   integer(c_int) function ecg_energy_ga(ctx, nmin, nmax, needed, which, want_vector, energy, nfact) &
@@ -246,6 +257,27 @@ subroutine GPU_EvalTrials(nfru, NTrials, ParSets, Energies, ErrorCodes)
   Glob_InvItTempCounter1 = Glob_InvItTempCounter1 + NTrials
   Glob_InvItTempCounter2 = Glob_InvItTempCounter2 + sum(iters)
 end subroutine GPU_EvalTrials
+
+!The energy + gradient of a newly added function (EnergyIB with nfru = nbase,
+!nfa = nbase+1, src/workproc.f90:2063-2154, as BasisEnlI's DRMNG loop calls
+!it, :4137-4170) for NTrials candidate parameter sets at once: Energies(i),
+!Gradients(1:npt,i) and ErrorCodes(i) are what EnergyIB returns once
+!ParSets(1:npt,i) is function nbase+1.  The basis of nbase functions must be
+!current on the device; it is left unchanged.
+subroutine GPU_EvalTrialsGrad(nbase, NTrials, ParSets, Energies, Gradients, ErrorCodes)
+  integer, intent(in) :: nbase, NTrials
+  real(dprec), intent(in) :: ParSets(Glob_npt, NTrials)
+  real(dprec), intent(out) :: Energies(NTrials), Gradients(Glob_npt, NTrials)
+  integer, intent(out) :: ErrorCodes(NTrials)
+  integer(c_int) :: st, codes(NTrials), iters(NTrials)
+  real(c_double) :: relacc(NTrials)
+  st = ecg_eval_candidates_grad(ecg_ctx, nbase, NTrials, ParSets, Glob_ApproxEnergy, Glob_EigvalTol, &
+                                Glob_MaxIterForGHEPIIS, Energies, codes, iters, relacc, Gradients)
+  if (st /= 0) stop 'GPU_EvalTrialsGrad: ecg_eval_candidates_grad failed'
+  ErrorCodes = codes
+  Glob_InvItTempCounter1 = Glob_InvItTempCounter1 + NTrials
+  Glob_InvItTempCounter2 = Glob_InvItTempCounter2 + sum(iters)
+end subroutine GPU_EvalTrialsGrad
 
 !EnergyGA (WantVector=.false.) / EnergyGAM (.true.), src/workproc.f90:1697,
 !for a context created with Glob_GSEPSolutionMethod='G': the

@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--cpu-baseline", type=int, default=1)
     ap.add_argument("--candidates", type=int, default=1, help="also time the batched-candidate configuration")
+    ap.add_argument("--composite", type=int, default=1,
+                    help="also time one new function's energy + gradient at K: plain, adjoint, batched")
     ap.add_argument("--cand-K", type=int, default=2000)
     ap.add_argument("--expc", type=int, default=1, help="also time the expectation-value pass")
     ap.add_argument("--expc-K", type=int, default=4000)
@@ -402,6 +404,11 @@ def run_ours(args, dist):
         line["cpu_baseline"] = cpu_sample(sysm, sets, lam, K, args.tol, max(1, int(np.ceil(np.mean(iters)))),
                                           warmup=1, steps=2)
     ctx.close()
+    if args.composite:
+        comp = run_composite(args, dev, dist.rank, lam)
+        comp["full_gradient"] = {"adjoint_ms": ms_step, "plain_ms": plain["ms_per_step"] if plain else None,
+                                 "speedup": (plain["ms_per_step"] / ms_step) if plain else None}
+        line["north_star"] = comp
     if args.candidates:
         line["candidates"] = run_candidates(args, dev, dist.rank, cpu=bool(args.cpu_baseline and dist.rank == 0))
     if args.expc:
@@ -418,7 +425,7 @@ def cpu_sample(sysm, sets, lam, K, tol, max_iter, warmup=1, steps=2, start=0):
     the GPU steps.  Returns the cpu_baseline object (value in evals/s)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
-    threads = os.cpu_count() or 1
+    threads = orc.host_threads()
     orc.set_threads(threads)
     orc.set_ldlhf_mode(-1)
     o = orc.Oracle(sysm, K, max_nfo=K)
@@ -441,6 +448,83 @@ def cpu_sample(sysm, sets, lam, K, tol, max_iter, warmup=1, steps=2, start=0):
                        f"LDLHF {'parallel' if par else 'serial'} branch"),
             "seconds_per_eval": t, "seconds": [round(x, 3) for x in times], "invit_iters": its,
             "energies": Es, "cpu": platform.processor() or platform.machine()}
+
+
+def run_composite(args, dev, rank, lam):
+    """Energy + gradient of one new basis function at K = 4000 (n = 3, T = 4):
+    the evaluation the optimisation of a newly added function repeats
+    (BasisEnlI's DRMNG loop, src/workproc.f90:4137-4170; OptCycleI): the
+    first K-1 functions of the seed-1002 basis are fixed and factorised, the
+    candidate is function K.  Three ways, all through the C ABI with host
+    buffers:
+      plain     per candidate ecg_set_params + ecg_energy_ib(K-1, K): row K
+                with derivatives into Glob_D, GHEPIIS(K, K) on the base
+                factor, the Glob_D contraction (the reference's sequence);
+      adjoint   per candidate ecg_set_params + ecg_energy_ib_adjoint(K-1, K);
+      batched   ecg_eval_candidates_grad for 256 candidates at once (bordered
+                Schur-complement inverse iteration for all candidates, the
+                fused adjoint pass over their rows).
+    Candidates follow GenerateTrialParam's rule from the base functions."""
+    from ecg_b200 import Context, synth
+    K = args.K or 4000
+    K0 = K - 1
+    sysm, params = synth.config_basis(CONFIG_INDEX, K=K)
+    base = params[:K0]
+    B = 256
+    cands = synth.candidates(base, B, 3002 + 7919 * rank)
+    tol = args.tol
+    with Context(sysm, K, max_nfo=1, device=dev) as ctx:
+        ctx.set_params(base)
+        ctx.set_vectors(K0, last_eigvec=np.ones(K0, dtype=np.complex128))
+        E0, err0, it0 = ctx.energy_ia(1, K0, lam, tol, max_iter=50)
+        _, x = ctx.vectors(K)
+        start = x.copy()
+        start[K0] = 0.0
+        out = {"workload": f"energy + gradient of function K={K} (n=3, T=4) against a fixed, factorised base of "
+                           f"{K0}; {B} candidates (GenerateTrialParam rule), tol {tol:g}",
+               "base_energy": E0}
+        nsing = 16
+        for mode in ("plain", "adjoint"):
+            fn = ctx.energy_ib if mode == "plain" else ctx.energy_ib_adjoint
+            ctx.set_params(cands[:1], first=K)
+            ctx.set_vectors(K, last_eigvec=start)
+            fn(K0, K, lam, tol)  # warm-up (graphs, workspaces)
+            ms, its = 0.0, []
+            for j in range(nsing):
+                ctx.set_vectors(K, last_eigvec=start)
+                ctx.timer_start()
+                ctx.set_params(cands[j:j + 1], first=K)
+                Ej, gj, ej, itj = fn(K0, K, lam, tol)
+                ms += ctx.timer_stop()
+                its.append(itj)
+            out[mode] = {"ms_per_eval": ms / nsing, "evals_per_s": nsing / (ms / 1e3),
+                         "invit_iters": float(np.mean(its)), "sample": nsing}
+        ctx.set_vectors(K, last_eigvec=start)
+        ctx.eval_candidates_grad(K0, cands, lam, tol)  # warm-up
+        reps, ms = 3, 0.0
+        for _ in range(reps):
+            ctx.set_vectors(K, last_eigvec=start)
+            ctx.timer_start()
+            E, err, it, ra, g = ctx.eval_candidates_grad(K0, cands, lam, tol)
+            ms += ctx.timer_stop()
+        ms /= reps
+        out["batched"] = {"ms_per_call": ms, "candidates_per_call": B, "ms_per_eval": ms / B,
+                          "evals_per_s": B / (ms / 1e3), "codes": np.bincount(err, minlength=3).tolist(),
+                          "iterations": np.bincount(it).tolist()}
+        # the batched results against the one-call adjoint path on a few candidates
+        diffs = []
+        for j in range(4):
+            if err[j] != 0:
+                continue
+            ctx.set_params(cands[j:j + 1], first=K)
+            ctx.set_vectors(K, last_eigvec=start)
+            Ej, gj, ej, _ = ctx.energy_ib_adjoint(K0, K, lam, tol)
+            diffs.append((abs(Ej - E[j]), float(np.max(np.abs(gj - g[j])) / np.max(np.abs(gj)))))
+        out["batched_vs_single"] = {"max_abs_dE": max(d[0] for d in diffs) if diffs else None,
+                                    "max_rel_dgrad": max(d[1] for d in diffs) if diffs else None}
+    out["speedup_batched_vs_plain"] = out["plain"]["ms_per_eval"] / out["batched"]["ms_per_eval"]
+    out["speedup_adjoint_vs_plain"] = out["plain"]["ms_per_eval"] / out["adjoint"]["ms_per_eval"]
+    return out
 
 
 def run_candidates(args, dev, rank, cpu=True):
@@ -507,7 +591,7 @@ def cpu_candidates(sysm, params, cands, K0, Kp=600, ntrial=8):
     iterations)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
-    threads = os.cpu_count() or 1
+    threads = orc.host_threads()
     orc.set_threads(threads)
     o = orc.Oracle(sysm, Kp + 1)
     o.set_params(params[:Kp])
@@ -567,7 +651,7 @@ def cpu_expc(sysm, params, terms, Kp=300):
     K' functions, scaled to the full pair count."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
-    threads = os.cpu_count() or 1
+    threads = orc.host_threads()
     orc.set_threads(threads)
     o = orc.Oracle(sysm, Kp)
     o.set_params(params[:Kp])

@@ -256,6 +256,13 @@ int ecg_sync(ecg_ctx* ctx);
  * records a second one, waits for it and returns the elapsed ms. */
 int ecg_timer_start(ecg_ctx* ctx);
 int ecg_timer_stop(ecg_ctx* ctx, double* ms);
+/* Poll limit of the bounded device waits in the context's triangular
+ * solves (GHEPIIS and the batched candidates): every wait on another CTA's
+ * panel gives up after `polls` polls (about 64 ns each), records the
+ * timeout and the call returns ECG_ECUDA with the context still usable.
+ * polls < 0 restores the default (2^22).  No counterpart in the reference:
+ * a diagnostic that lets a test make a wait run out without a fault. */
+int ecg_set_wait_limit(ecg_ctx* ctx, int polls);
 /* Bytes this context has copied host->device and device->host so far. */
 int ecg_io_bytes(ecg_ctx* ctx, long long* h2d, long long* d2h);
 /* The fused adjoint gradient of ecg_energy_ib_adjoint, for callers that

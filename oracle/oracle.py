@@ -66,12 +66,28 @@ def load():
         lib.orc_overlap_penalty.restype = C.c_double
         lib.orc_set_threads.argtypes = [C.c_int]
         lib.orc_get_threads.restype = C.c_int
+        lib.orc_set_threads(host_threads())
         _lib = lib
     return _lib
 
 
 def _p(a):
     return a.ctypes.data_as(_dp)
+
+
+def host_threads():
+    """CPUs this process can use: its affinity mask, capped by a cgroup CPU
+    quota when one is set (an OpenMP team larger than the quota
+    oversubscribes the cores, which the parallel LDLHF branch's per-chunk
+    barriers do not tolerate)."""
+    n = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        quota, period = open("/sys/fs/cgroup/cpu.max").read().split()[:2]
+        if quota != "max":
+            n = min(n, max(1, int(int(quota) // int(period))))
+    except (OSError, ValueError):
+        pass
+    return max(1, n)
 
 
 def set_threads(n):
