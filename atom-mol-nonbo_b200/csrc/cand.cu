@@ -476,10 +476,11 @@ enum { BR_V = 0, BR_W = 1, BR_INVD = 2, BR_X = 3 };
 
 // Bordered LDLHF step for row K (src/linalg.f90:359-383):
 // x = M(K,K) - sum_q conj(a_q) U(q,K);  d_K = conj(x);  invD_K = 1/d_K,
-// with the pivot's rounding-level imaginary part dropped (k_ldl_diag).
+// with the pivot's rounding-level imaginary part dropped (cplx = 0, as in
+// k_ldl_diag<false>) or kept (cplx = 1, as the reference keeps it).
 __global__ void __launch_bounds__(256) k_cand_border(const cd* __restrict__ Acol, const cd* __restrict__ Lcol,
                                                      const double* __restrict__ mu, int nbase, int ldv, int bcap,
-                                                     cd* __restrict__ brd, int* __restrict__ st)
+                                                     cd* __restrict__ brd, int* __restrict__ st, int cplx)
 {
     __shared__ double sh[8 * 2];
     const int j = blockIdx.x;
@@ -493,13 +494,16 @@ __global__ void __launch_bounds__(256) k_cand_border(const cd* __restrict__ Acol
     }
     block_sum256<2>(v, sh);
     if (threadIdx.x == 0) {
-        // real pivot, as in k_ldl_diag: Im(sum) is rounding noise
-        const double x = mu[j] - v[0];
-        if (x == 0.0) {
+        const double xr = mu[j] - v[0];
+        const double xi = cplx ? v[1] : 0.0;  // d_K = conj(x): Im d_K = +Im(sum)
+        if (xr == 0.0 && xi == 0.0) {
             st[ST_ERR * bcap + j] = 1;
             brd[BR_INVD * bcap + j] = mk(0.0, 0.0);
+        } else if (!cplx) {
+            brd[BR_INVD * bcap + j] = mk(1.0 / xr, 0.0);
         } else {
-            brd[BR_INVD * bcap + j] = mk(1.0 / x, 0.0);
+            const double m = 1.0 / fma(xr, xr, xi * xi);
+            brd[BR_INVD * bcap + j] = mk(xr * m, -xi * m);
         }
     }
 }
@@ -1044,7 +1048,8 @@ int eval_candidates(Ctx& c, int nbase, int count, const double* cand_host, doubl
     }
     // bordered factor row: Acol = L0^-1 Mcol, Lcol = invD o Acol, then d_K
     if (launch_solve(c, true, nb, ncols, cw.Mcol, cw.Acol, cw.Lcol, nullptr)) return ECG_ECUDA;
-    k_cand_border<<<count, 256, 0, c.stream>>>(cw.Acol, cw.Lcol, cw.mu, nbase, cw.ldv, cc, cw.brd, cw.st);
+    k_cand_border<<<count, 256, 0, c.stream>>>(cw.Acol, cw.Lcol, cw.mu, nbase, cw.ldv, cc, cw.brd, cw.st,
+                                               c.pivot_mode);
     {
         dim3 g((nbase + 255) / 256, ncols);
         if (g.x > 16) g.x = 16;

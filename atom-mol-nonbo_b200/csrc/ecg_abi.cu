@@ -574,6 +574,19 @@ int ecg_set_params_device(ecg_ctx* ctx, const double* params_dev, int first, int
     return ECG_OK;
 }
 
+int ecg_set_pivot_mode(ecg_ctx* ctx, int mode)
+{
+    if (!ctx || mode < 0 || mode > 1) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (c.pivot_mode != mode) {
+        c.pivot_mode = mode;
+        // a factor made with the other pivots is not reused
+        c.fact_n = 0;
+        c.blk_start.clear();
+    }
+    return ECG_OK;
+}
+
 int ecg_set_wait_limit(ecg_ctx* ctx, int polls)
 {
     if (!ctx) return ECG_EARG;

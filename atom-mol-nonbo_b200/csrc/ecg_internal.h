@@ -142,6 +142,7 @@ struct Ctx {
     double* red_h = nullptr;    // pinned host mirror of the reduction results
     int* counters = nullptr;    // last-block counters [0,1], abort word [2], wait poll limit [3] of the solves
     int wait_limit = SOLVE_SPIN_LIMIT;
+    int pivot_mode = 0;         // LDL^H pivots: 0 real (default), 1 complex as the reference keeps them
     cd* yv = nullptr;           // forward-solve result (ld)
     cd* zv = nullptr;           // D^-1 scaled forward result (ld)
     cd* spart = nullptr;        // per-CTA partial sums of the blocked solves

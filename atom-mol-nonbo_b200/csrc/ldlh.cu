@@ -80,15 +80,19 @@ constexpr int DG_LD = LDL_NB + 1;
 // r mod 32 of warp c mod 8 (two rows and eight columns per thread, so the
 // loads and stores of a warp are whole column segments).  Per pivot q the
 // eight threads holding row q publish it to shared memory; after one
-// barrier every thread reads the pivot d = W(q, q) (real: the imaginary
-// part of W(q, q) is rounding noise of the updates; kept, it sets a floor
-// of 1e-13..1e-12 under GHEPIIS's residual NormOfDiff), and applies the
-// rank-one update W(r, c) -= conj(U(q, r)) Wun(q, c), U(q, r) = Wun(q, r)/d,
-// to its elements with q < r <= c; the row-q holders scale their row to
-// U(q, c).  Column groups beyond q are tested per warp, the rows below 32
-// per block, so finished parts cost no issue slots.  The recurrence and
-// the pivot d = conj(W(q, q)) follow src/linalg.f90:359-391; only the
-// summation order differs from the reference's row-by-row dot products.
+// barrier every thread reads the pivot d = W(q, q) and applies the rank-one
+// update W(r, c) -= conj(U(q, r)) Wun(q, c), U(q, r) = Wun(q, r)/d, to its
+// elements with q < r <= c; the row-q holders scale their row to U(q, c).
+// Column groups beyond q are tested per warp, the rows below 32 per block,
+// so finished parts cost no issue slots.  The recurrence follows
+// src/linalg.f90:359-391: W(q, q) accumulated this way is the reference's
+// pivot conj(x) (M(q, q) is real), zero test included; only the summation
+// order differs from the reference's row-by-row dot products.
+// CPLX = false (default): the pivot's imaginary part, rounding noise of
+// the updates, is dropped (kept, it sets a floor of 1e-13..1e-12 under
+// GHEPIIS's residual NormOfDiff); true: the complex pivot is kept, as the
+// reference keeps it.
+template <bool CPLX>
 __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, int p0, int p1, cd* __restrict__ dw,
                                                    cd* __restrict__ invD, int* __restrict__ status)
 {
@@ -117,18 +121,33 @@ __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, in
                 }
         }
         __syncthreads();
-        const double d = rb[buf][q].x;
-        const double inv = (d != 0.0) ? __drcp_rn(d) : 0.0;
+        const double2 dq = rb[buf][q];
+        double inv, invi = 0.0;  // 1 / d
+        bool zero;
+        if (CPLX) {
+            zero = (dq.x == 0.0 && dq.y == 0.0);
+            const double m = zero ? 0.0 : __drcp_rn(fma(dq.x, dq.x, dq.y * dq.y));
+            inv = dq.x * m;
+            invi = -dq.y * m;
+        } else {
+            zero = (dq.x == 0.0);
+            inv = zero ? 0.0 : __drcp_rn(dq.x);
+        }
         if (threadIdx.x == 0) {
-            invD[p0 + q] = cd{inv, 0.0};
-            if (d == 0.0) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + q + 1);
+            invD[p0 + q] = cd{inv, invi};
+            if (zero) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + q + 1);
         }
         double ur[2], ui[2];
 #pragma unroll
         for (int j = 0; j < 2; j++) {
-            const double2 u = rb[buf][lane + 32 * j];  // conj(U(q, r)) = conj(Wun(q, r)) / d
-            ur[j] = u.x * inv;
-            ui[j] = -u.y * inv;
+            const double2 u = rb[buf][lane + 32 * j];  // conj(U(q, r)) = conj(Wun(q, r) / d)
+            if (CPLX) {
+                ur[j] = fma(u.x, inv, -u.y * invi);
+                ui[j] = -fma(u.x, invi, u.y * inv);
+            } else {
+                ur[j] = u.x * inv;
+                ui[j] = -u.y * inv;
+            }
         }
 #pragma unroll
         for (int a = 0; a < 8; a++) {
@@ -143,8 +162,14 @@ __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, in
                         wr[j][a] = fma(-ur[j], v.x, fma(ui[j], v.y, wr[j][a]));
                         wi[j][a] = fma(-ur[j], v.y, fma(-ui[j], v.x, wi[j][a]));
                     } else if (r == q) {
-                        wr[j][a] *= inv;
-                        wi[j][a] *= inv;
+                        if (CPLX) {
+                            const double x = wr[j][a], y = wi[j][a];
+                            wr[j][a] = fma(x, inv, -y * invi);
+                            wi[j][a] = fma(x, invi, y * inv);
+                        } else {
+                            wr[j][a] *= inv;
+                            wi[j][a] *= inv;
+                        }
                     }
                 }
             }
@@ -427,7 +452,10 @@ static void enqueue_factor(Ctx& c, int m0, int n, const std::vector<int>& starts
         c.launches++;
     };
     auto diag = [&](int p0, int p1) {
-        k_ldl_diag<<<1, 256, 0, c.stream>>>(c.F, c.ld, p0, p1, c.dw, c.invD, c.status);
+        if (c.pivot_mode)
+            k_ldl_diag<true><<<1, 256, 0, c.stream>>>(c.F, c.ld, p0, p1, c.dw, c.invD, c.status);
+        else
+            k_ldl_diag<false><<<1, 256, 0, c.stream>>>(c.F, c.ld, p0, p1, c.dw, c.invD, c.status);
         c.launches++;
     };
     if (n > m0) {
@@ -525,7 +553,7 @@ int ldlh_factor(Ctx& c, int m0, int n)
     if (cudaMemcpyAsync(c.dblk, c.bounds_h, (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, c.stream) !=
         cudaSuccess)
         return -2;
-    std::vector<int> key = {m0, n};
+    std::vector<int> key = {m0, n, c.pivot_mode};
     key.insert(key.end(), starts.begin(), starts.begin() + nexist);
     Ctx::LdlGraph* g = nullptr;
     for (auto& e : c.ldl_graphs)

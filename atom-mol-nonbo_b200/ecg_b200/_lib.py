@@ -51,6 +51,7 @@ PROTOTYPES = {
     "ecg_sync": (C.c_int, [_vp]),
     "ecg_timer_start": (C.c_int, [_vp]),
     "ecg_timer_stop": (C.c_int, [_vp, _dp]),
+    "ecg_set_pivot_mode": (C.c_int, [_vp, C.c_int]),
     "ecg_set_wait_limit": (C.c_int, [_vp, C.c_int]),
     "ecg_io_bytes": (C.c_int, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "ecg_probe_fp64_peak": (C.c_int, [C.c_int, _dp]),

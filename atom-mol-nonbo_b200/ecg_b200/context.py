@@ -358,6 +358,10 @@ class Context:
         _check(self.lib.ecg_timer_stop(self.h, C.byref(ms)), "ecg_timer_stop")
         return ms.value
 
+    def set_pivot_mode(self, mode):
+        """LDL^H pivots: 0 real (default), 1 complex as the reference."""
+        _check(self.lib.ecg_set_pivot_mode(self.h, int(mode)), "ecg_set_pivot_mode")
+
     def set_wait_limit(self, polls):
         """Poll limit of the solves' bounded device waits (< 0: default)."""
         _check(self.lib.ecg_set_wait_limit(self.h, int(polls)), "ecg_set_wait_limit")

@@ -256,6 +256,16 @@ int ecg_sync(ecg_ctx* ctx);
  * records a second one, waits for it and returns the elapsed ms. */
 int ecg_timer_start(ecg_ctx* ctx);
 int ecg_timer_stop(ecg_ctx* ctx, double* ms);
+/* Pivots of the context's LDL^H factorisations (GHEPIIS, the candidates'
+ * bordered step, the 'G' path): mode 0 (default) keeps them real, dropping
+ * the rounding-level imaginary part that the complex arithmetic of
+ * LDLHF (src/linalg.f90:370-381) leaves in them; mode 1 keeps the complex
+ * pivot d = conj(x) and its exact x == 0 test as the reference does.  The
+ * energies agree to rounding either way; the imaginary parts set a floor
+ * of about 1e-13..1e-12 under GHEPIIS's NormOfDiff, so near
+ * EIGVAL_TOLERANCE = 1e-12 mode 1 returns ErrorCode 2 where the reference
+ * does and mode 0 converges.  Changing the mode discards the factor. */
+int ecg_set_pivot_mode(ecg_ctx* ctx, int mode);
 /* Poll limit of the bounded device waits in the context's triangular
  * solves (GHEPIIS and the batched candidates): every wait on another CTA's
  * panel gives up after `polls` polls (about 64 ns each), records the

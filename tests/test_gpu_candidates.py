@@ -88,6 +88,31 @@ def test_candidates_match_oracle(cfg, K0, B, seed, factor_base, tol):
         assert np.array_equal(gpu[1], ref[1])
 
 
+@pytest.mark.parametrize("cfg,K0,B,seed", [(1, 200, 70, 11), (4, 100, 17, 13)])
+def test_complex_pivot_mode_at_the_reference_tolerance(cfg, K0, B, seed):
+    """Pivot mode 1 keeps the complex LDL^H pivots as the reference does
+    (src/linalg.f90:370-381).  At EIGVAL_TOLERANCE 1e-12, where the oracle's
+    residual floor decides the ErrorCode, the GPU's codes are compared with
+    the oracle's candidate by candidate; the energies agree to 1e-10."""
+    tol = 1e-12
+    sysm, params, cands, o, lam, start = base_problem(cfg, K0, B, seed)
+    ref = o.trial_loop(K0, cands, lam, tol, start)
+    with Context(sysm, K0 + 1) as ctx:
+        ctx.set_pivot_mode(1)
+        ctx.set_params(params)
+        ctx.set_vectors(K0, last_eigvec=np.ones(K0, dtype=np.complex128))
+        ctx.energy_ia(1, K0, lam, tol)
+        ctx.set_vectors(K0 + 1, last_eigvec=start)
+        E, err, it, ra = ctx.eval_candidates(K0, cands, lam, tol)
+    Eo, erro, ito, rao = ref
+    ok = (err != 1) & (erro != 1)
+    print(f"cfg {cfg} complex pivots: codes gpu {np.bincount(err, minlength=3)} oracle "
+          f"{np.bincount(erro, minlength=3)}; equal {np.mean(err == erro) * 100:.0f}%; residual median gpu "
+          f"{np.median(ra):.2e} oracle {np.median(rao):.2e}; max |dE| {np.max(np.abs(E - Eo)[ok]):.2e}")
+    assert np.all(np.abs(E - Eo)[ok] <= TOL_E)
+    assert np.array_equal(err, erro)
+
+
 def test_candidates_negative_tol_and_iteration_limit():
     """Tol < 0 (iterate until the residual stops decreasing) and MaxIter = 2
     (ErrorCode 2 for candidates still iterating), as GHEPIIS defines them.
