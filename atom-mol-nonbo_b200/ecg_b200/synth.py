@@ -96,6 +96,13 @@ CONFIGS = {
 }
 
 
+# configs[4] names "5 particles: one heavy particle and three electrons,
+# n = 4": the particle list describes the n = 3 Li-like system of
+# CONFIGS[4]; the five-particle n = 4 reading is this one (heavy particle
+# and four electrons), with the same seed, size and mass scaling.
+CONFIG4_N4 = dict(system="li_minus_like", K=10000, seed=1004, mass_scaled=True)
+
+
 def systems():
     """The physical systems of the benchmark configurations."""
     return SYSTEMS
@@ -115,9 +122,10 @@ def reduced_mass_scale(masses):
 
 
 def config_basis(index, K=None):
-    """(system, params) of benchmark configuration `index`; K overrides the
-    basis size (the first K functions of the full basis are the same)."""
-    cfg = CONFIGS[index]
+    """(system, params) of benchmark configuration `index` (or "4n4" for
+    CONFIG4_N4); K overrides the basis size (the first K functions of the
+    full basis are the same)."""
+    cfg = CONFIG4_N4 if index == "4n4" else CONFIGS[index]
     sysm = make_system(cfg["system"])
     KK = cfg["K"] if K is None else K
     scale = reduced_mass_scale(SYSTEMS[cfg["system"]]["masses"]) if cfg.get("mass_scaled") else None

@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--cpu-baseline", type=int, default=1)
     ap.add_argument("--candidates", type=int, default=1, help="also time the batched-candidate configuration")
+    ap.add_argument("--large", type=int, default=1, help="also run configs[4]'s K=10000 step (n=3 and n=4)")
+    ap.add_argument("--large-K", type=int, default=10000)
     ap.add_argument("--composite", type=int, default=1,
                     help="also time one new function's energy + gradient at K: plain, adjoint, batched")
     ap.add_argument("--cand-K", type=int, default=2000)
@@ -409,6 +411,8 @@ def run_ours(args, dist):
         comp["full_gradient"] = {"adjoint_ms": ms_step, "plain_ms": plain["ms_per_step"] if plain else None,
                                  "speedup": (plain["ms_per_step"] / ms_step) if plain else None}
         line["north_star"] = comp
+    if args.large:
+        line["configs4_k10000"] = run_large(args, dev, dist.rank)
     if args.candidates:
         line["candidates"] = run_candidates(args, dev, dist.rank, cpu=bool(args.cpu_baseline and dist.rank == 0))
     if args.expc:
@@ -524,6 +528,47 @@ def run_composite(args, dev, rank, lam):
                                     "max_rel_dgrad": max(d[1] for d in diffs) if diffs else None}
     out["speedup_batched_vs_plain"] = out["plain"]["ms_per_eval"] / out["batched"]["ms_per_eval"]
     out["speedup_adjoint_vs_plain"] = out["plain"]["ms_per_eval"] / out["adjoint"]["ms_per_eval"]
+    return out
+
+
+def run_large(args, dev, rank):
+    """configs[4], K = 10000: one full energy + gradient step (H, S build,
+    LDL^H, inverse iteration at Tol 1e-12, fused adjoint gradient) for the
+    Li-like n = 3 system (six Y^+Y terms) and for the five-particle n = 4
+    system (heavy particle + four electrons, 14 terms), mass-scaled seeded
+    bases.  lambda~ = E * INVITPARAMETER from a first solve."""
+    from ecg_b200 import Context, synth
+    K = args.large_K
+    out = {}
+    for key, idx in (("n3_li_like", 4), ("n4_five_particles", "4n4")):
+        cfg = synth.CONFIG4_N4 if idx == "4n4" else synth.CONFIGS[idx]
+        sysm, params = synth.config_basis(idx, K=K)
+        if rank:
+            params = synth.random_basis(sysm.n, K, cfg["seed"] + 7919 * rank,
+                                        row_scale=synth.reduced_mass_scale(sysm.masses))
+        e_floor = synth.SYSTEMS[cfg["system"]]["e_floor"]
+        with Context(sysm, K, device=dev) as ctx:
+            ctx.set_params(params)
+            ctx.set_vectors(K, last_eigvec=np.ones(K, dtype=np.complex128))
+            E0, err0, it0 = ctx.energy_ia(1, K, e_floor, -1e-12, max_iter=300, specif_norm=0)
+            lam = E0 * INVIT_PARAMETER
+            ctx.energy_ia(1, K, lam, 1e-12, max_iter=50, specif_norm=0)
+            ctx.set_timing(True)
+            ctx.energy_ib_adjoint(0, K, lam, 1e-12)  # warm-up (graphs, workspaces)
+            reps, ms, st, its = 2, 0.0, np.zeros(4), []
+            for _ in range(reps):
+                ctx.timer_start()
+                E, g, err, it = ctx.energy_ib_adjoint(0, K, lam, 1e-12)
+                ms += ctx.timer_stop()
+                st += ctx.stage_ms()
+                its.append(int(it))
+            ctx.set_timing(False)
+        out[key] = {"n": sysm.n, "T": sysm.T, "K": K, "ms_per_step": ms / reps,
+                    "stages_ms": dict(zip(["pairs_hs", "ldlh", "invit", "adjoint"], (st / reps).round(3).tolist())),
+                    "energy": E, "error_code": int(err), "invit_iters": its, "lambda_tilde": lam,
+                    "search": {"E0": E0, "code": int(err0), "iters": int(it0)},
+                    "grad_norm": float(np.linalg.norm(g)),
+                    "ldlh_tflops": 4.0 / 3.0 * K ** 3 / (st[1] / reps * 1e-3) / 1e12}
     return out
 
 
