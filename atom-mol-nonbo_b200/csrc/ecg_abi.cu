@@ -574,6 +574,82 @@ int ecg_set_params_device(ecg_ctx* ctx, const double* params_dev, int first, int
     return ECG_OK;
 }
 
+int ecg_pair_tiles(ecg_ctx* ctx, int nmin, int nmax, long long* ntiles)
+{
+    if (!ctx || !ntiles || nmin < 1 || nmax < nmin || nmax > ctx->c.ld) return ECG_EARG;
+    *ntiles = tile_count((nmin - 1) / TILE, (nmax + TILE - 1) / TILE);
+    return ECG_OK;
+}
+
+static bool tile_range_ok(Ctx& c, int nmin, int nmax, long long first, long long count)
+{
+    if (nmin < 1 || nmax < nmin || nmax > c.ld || first < 0 || count < 0) return false;
+    return first + count <= tile_count((nmin - 1) / TILE, (nmax + TILE - 1) / TILE) && count < (1LL << 31);
+}
+
+int ecg_compute_mat_elem_tiles(ecg_ctx* ctx, int nmin, int nmax, double approx_energy, long long first,
+                               long long count)
+{
+    if (!ctx) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (!tile_range_ok(c, nmin, nmax, first, count)) return ECG_EARG;
+    CKR(launch_prep(c, nmax));
+    CKR(launch_pair_diag(c, nmin - 1, nmax, approx_energy, 0, 0));
+    CKR(launch_pair_energy_tiles(c, nmin - 1, nmax, approx_energy, first, count));
+    return ECG_OK;
+}
+
+int ecg_pack_tiles(ecg_ctx* ctx, int nmin, int nmax, long long first, long long count, void* packed_dev)
+{
+    if (!ctx || (!packed_dev && count > 0)) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (!tile_range_ok(c, nmin, nmax, first, count)) return ECG_EARG;
+    CKR(launch_tiles_copy(c, nmin - 1, nmax, first, count, static_cast<cd*>(packed_dev), 0));
+    return ECG_OK;
+}
+
+int ecg_unpack_tiles(ecg_ctx* ctx, int nmin, int nmax, long long first, long long count, const void* packed_dev)
+{
+    if (!ctx || (!packed_dev && count > 0)) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (!tile_range_ok(c, nmin, nmax, first, count)) return ECG_EARG;
+    CKR(launch_tiles_copy(c, nmin - 1, nmax, first, count, static_cast<cd*>(const_cast<void*>(packed_dev)), 1));
+    return ECG_OK;
+}
+
+int ecg_adjoint_part_doubles(ecg_ctx* ctx, long long* per_tile)
+{
+    if (!ctx || !per_tile) return ECG_EARG;
+    *per_tile = 2LL * TILE * adjoint_nv(ctx->c.n);
+    return ECG_OK;
+}
+
+int ecg_adjoint_tiles(ecg_ctx* ctx, int nfru, int nfa, double energy, long long first, long long count,
+                      void* part_dev)
+{
+    if (!ctx || (!part_dev && count > 0)) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (nfru < 0 || !tile_range_ok(c, nfru + 1, nfa, first, count)) return ECG_EARG;
+    CKR(launch_adjoint_tiles(c, nfru, nfa, energy, c.x, first, count, static_cast<double*>(part_dev)));
+    return ECG_OK;
+}
+
+int ecg_adjoint_finish(ecg_ctx* ctx, int nfru, int nfa, const void* part_dev, double* grad_host)
+{
+    if (!ctx || !part_dev) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (nfru < 0 || nfa <= nfru || nfa > c.ld) return ECG_EARG;
+    CKR(launch_adjoint_finish(c, nfru, nfa, static_cast<const double*>(part_dev)));
+    if (grad_host) {
+        const int nfo = nfa - nfru;
+        CK(cudaMemcpyAsync(grad_host, c.grad, (size_t)nfo * c.npt * sizeof(double), cudaMemcpyDeviceToHost,
+                           c.stream));
+        c.bytes_d2h += (long long)nfo * c.npt * sizeof(double);
+    }
+    CK(cudaStreamSynchronize(c.stream));
+    return ECG_OK;
+}
+
 int ecg_set_pivot_mode(ecg_ctx* ctx, int mode)
 {
     if (!ctx || mode < 0 || mode > 1) return ECG_EARG;

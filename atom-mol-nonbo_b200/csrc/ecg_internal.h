@@ -209,6 +209,15 @@ int launch_term_batch(Ctx& c, int count, const double* pk, const double* pl, con
                       cd* hs, cd* dk, cd* dl);
 
 int launch_cand_rows(Ctx& c, CandWork& cw, int nbase, int count, double approx_e, int variant);
+// Pair tiles split over ranks: a range of the off-diagonal tile list of
+// rows [r0, r1) (tile_count order), its packing, and the adjoint pass over
+// a range with the gradient from all partials.
+int launch_pair_energy_tiles(Ctx& c, int r0, int r1, double approx_e, long long t0, long long count);
+int launch_tiles_copy(Ctx& c, int r0, int r1, long long t0, long long count, cd* buf, int dir);
+int launch_adjoint_tiles(Ctx& c, int nfru, int nfa, double E, const cd* cvec, long long t0, long long count,
+                         double* part);
+int launch_adjoint_finish(Ctx& c, int nfru, int nfa, const double* part);
+int adjoint_nv(int n);
 // Gradients of the candidates' energies with respect to their own
 // parameters from their final eigenpairs (border entry vK, x^H S x = t1).
 int launch_cand_adjoint(Ctx& c, CandWork& cw, int nbase, int count, const cd* vK, const double* t1,

@@ -269,11 +269,11 @@ __global__ void __launch_bounds__(256) k_pair_energy(SysParams sp, const double*
                                                      const double* __restrict__ detL,
                                                      const double* __restrict__ diagS, cd* __restrict__ H,
                                                      cd* __restrict__ S, int ld, int r0, int r1, int Rlo,
-                                                     char method, double approx_e)
+                                                     char method, double approx_e, long long t0)
 {
     constexpr int NP = Sym<N>::NP;
     int R, C;
-    tile_rc(blockIdx.x, Rlo, R, C);
+    tile_rc(t0 + blockIdx.x, Rlo, R, C);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int k = R * TILE + lane;
     if (k < r0 || k >= r1) return;
@@ -414,13 +414,14 @@ __global__ void __launch_bounds__(256) k_adjoint(SysParams sp, const double* __r
                                                  const double* __restrict__ Pd, const cd* __restrict__ bra,
                                                  const cd* __restrict__ ket, const double* __restrict__ detL,
                                                  const double* __restrict__ diagS, const cd* __restrict__ cvec,
-                                                 double E, int nfru, int nfa, int Rlo, double* __restrict__ part)
+                                                 double E, int nfru, int nfa, int Rlo, double* __restrict__ part,
+                                                 long long t0)
 {
     constexpr int NP = Sym<N>::NP;
     constexpr int NV = AdjNV<N>::value;
     extern __shared__ double red[];  // [8][32][NV]
     int R, C;
-    tile_rc(blockIdx.x, Rlo, R, C);
+    tile_rc(t0 + blockIdx.x, Rlo, R, C);
     const long long tile = blockIdx.x;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int k = R * TILE + lane;
@@ -1043,11 +1044,61 @@ static int energy_n(Ctx& c, int r0, int r1, double approx_e)
     const int Rlo = r0 / TILE, Rhi = (r1 + TILE - 1) / TILE;
     const long long nt = tile_count(Rlo, Rhi);
     k_pair_energy<N><<<(unsigned)nt, 256, 0, c.stream>>>(c.sp, c.coef, c.bra, c.ket, c.detL, c.diagS, c.H, c.S,
-                                                         c.ld, r0, r1, Rlo, c.method, approx_e);
+                                                         c.ld, r0, r1, Rlo, c.method, approx_e, 0LL);
     c.launches++;
     return last_err();
 }
 int launch_pair_energy(Ctx& c, int r0, int r1, double approx_e) { ECG_DISPATCH_N(c.n, energy_n, c, r0, r1, approx_e) }
+
+// Tiles [t0, t0 + count) of the list k_pair_energy walks for rows [r0, r1).
+template <int N>
+static int energy_tiles_n(Ctx& c, int r0, int r1, double approx_e, long long t0, long long count)
+{
+    if (r1 <= r0 || count <= 0) return 0;
+    const int Rlo = r0 / TILE;
+    k_pair_energy<N><<<(unsigned)count, 256, 0, c.stream>>>(c.sp, c.coef, c.bra, c.ket, c.detL, c.diagS, c.H, c.S,
+                                                            c.ld, r0, r1, Rlo, c.method, approx_e, t0);
+    c.launches++;
+    return last_err();
+}
+int launch_pair_energy_tiles(Ctx& c, int r0, int r1, double approx_e, long long t0, long long count)
+{
+    ECG_DISPATCH_N(c.n, energy_tiles_n, c, r0, r1, approx_e, t0, count)
+}
+
+// Pack (dir 0) or unpack (dir 1) the off-diagonal entries k > l, k in
+// [r0, r1), of tiles [t0, t0 + count) of that list: buf holds per tile H
+// then S as [l][k] 32 x 32 complex blocks; unpacking writes H(k,l), S(k,l)
+// and, in 'I' storage, S(l,k) = conj(S(k,l)), as k_pair_energy stores them.
+__global__ void __launch_bounds__(256) k_tiles_copy(cd* __restrict__ H, cd* __restrict__ S, int ld, int r0, int r1,
+                                                    int Rlo, long long t0, cd* __restrict__ buf, int dir, char method)
+{
+    int R, C;
+    tile_rc(t0 + blockIdx.x, Rlo, R, C);
+    cd* tb = buf + (size_t)blockIdx.x * 2 * TILE * TILE;
+    for (int e = threadIdx.x; e < TILE * TILE; e += blockDim.x) {
+        const int lk = e & 31, ll = e >> 5;
+        const int k = R * TILE + lk, l = C * TILE + ll;
+        if (k < r0 || k >= r1 || l >= k) continue;
+        const size_t kl = (size_t)k + (size_t)l * ld;
+        if (dir == 0) {
+            tb[e] = H[kl];
+            tb[TILE * TILE + e] = S[kl];
+        } else {
+            const cd sv = tb[TILE * TILE + e];
+            H[kl] = tb[e];
+            S[kl] = sv;
+            if (method == 'I') S[(size_t)l + (size_t)k * ld] = conj(sv);
+        }
+    }
+}
+int launch_tiles_copy(Ctx& c, int r0, int r1, long long t0, long long count, cd* buf, int dir)
+{
+    if (r1 <= r0 || count <= 0) return 0;
+    k_tiles_copy<<<(unsigned)count, 256, 0, c.stream>>>(c.H, c.S, c.ld, r0, r1, r0 / TILE, t0, buf, dir, c.method);
+    c.launches++;
+    return last_err();
+}
 
 template <int N>
 static int grad_n(Ctx& c, int r0, int r1, int nfru, double approx_e)
@@ -1096,7 +1147,7 @@ static int adjoint_n(Ctx& c, int nfru, int nfa, double E)
         attr = true;
     }
     k_adjoint<N><<<(unsigned)nt, 256, smem, c.stream>>>(c.sp, c.coef, c.Pd, c.bra, c.ket, c.detL, c.diagS, c.c, E,
-                                                        nfru, nfa, Rlo, c.part);
+                                                        nfru, nfa, Rlo, c.part, 0LL);
     c.launches++;
     const int nf = nfa - nfru;
     k_adjoint_final<N><<<(nf * 32 + 255) / 256, 256, 0, c.stream>>>(c.part, c.params, nfru, nfa, Rlo, Rhi, c.grad);
@@ -1104,6 +1155,46 @@ static int adjoint_n(Ctx& c, int nfru, int nfa, double E)
     return last_err();
 }
 int launch_adjoint(Ctx& c, int nfru, int nfa, double E) { ECG_DISPATCH_N(c.n, adjoint_n, c, nfru, nfa, E) }
+
+// The adjoint pass over tiles [t0, t0 + count) of its list only, with the
+// eigenvector cvec; part receives their partials (count x 2 x 32 x NV),
+// in the order the whole pass writes them.
+template <int N>
+static int adjoint_tiles_n(Ctx& c, int nfru, int nfa, double E, const cd* cvec, long long t0, long long count,
+                           double* part)
+{
+    if (nfa <= nfru || count <= 0) return 0;
+    constexpr int NV = AdjNV<N>::value;
+    const size_t smem = (size_t)8 * TILE * NV * sizeof(double);
+    if (cudaFuncSetAttribute(k_adjoint<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return -2;
+    k_adjoint<N><<<(unsigned)count, 256, smem, c.stream>>>(c.sp, c.coef, c.Pd, c.bra, c.ket, c.detL, c.diagS, cvec,
+                                                           E, nfru, nfa, nfru / TILE, part, t0);
+    c.launches++;
+    return last_err();
+}
+int launch_adjoint_tiles(Ctx& c, int nfru, int nfa, double E, const cd* cvec, long long t0, long long count,
+                         double* part)
+{
+    ECG_DISPATCH_N(c.n, adjoint_tiles_n, c, nfru, nfa, E, cvec, t0, count, part)
+}
+
+// The gradient from the partials of every tile of the list, in list order.
+template <int N>
+static int adjoint_finish_n(Ctx& c, int nfru, int nfa, const double* part)
+{
+    if (nfa <= nfru) return 0;
+    const int Rlo = nfru / TILE, Rhi = (nfa + TILE - 1) / TILE;
+    const int nf = nfa - nfru;
+    k_adjoint_final<N><<<(nf * 32 + 255) / 256, 256, 0, c.stream>>>(part, c.params, nfru, nfa, Rlo, Rhi, c.grad);
+    c.launches++;
+    return last_err();
+}
+int launch_adjoint_finish(Ctx& c, int nfru, int nfa, const double* part)
+{
+    ECG_DISPATCH_N(c.n, adjoint_finish_n, c, nfru, nfa, part)
+}
+int adjoint_nv(int n) { return 2 * (n * (n + 1) / 2) + 1; }
 
 int launch_plain_contract(Ctx& c, int nfo, int nfa, int nfru, double E)
 {
@@ -1293,7 +1384,8 @@ static int run(const SysParams& sp, const Terms& terms, unsigned char* base, con
         cudaGetLastError();
         return ECG_ECUDA;
     }
-    k_adjoint<N><<<(unsigned)nt, 256, smem, st>>>(sp, coef, Pd, bra, ket, detL, diagS, cvec, E, nfru, nfa, Rlo, part);
+    k_adjoint<N><<<(unsigned)nt, 256, smem, st>>>(sp, coef, Pd, bra, ket, detL, diagS, cvec, E, nfru, nfa, Rlo, part,
+                                                  0LL);
     const int nf = nfa - nfru;
     k_adjoint_final<N><<<(nf * 32 + 255) / 256, 256, 0, st>>>(part, params, nfru, nfa, Rlo, Rhi, grad);
     return cudaGetLastError() == cudaSuccess ? ECG_OK : ECG_ECUDA;

@@ -51,6 +51,13 @@ PROTOTYPES = {
     "ecg_sync": (C.c_int, [_vp]),
     "ecg_timer_start": (C.c_int, [_vp]),
     "ecg_timer_stop": (C.c_int, [_vp, _dp]),
+    "ecg_pair_tiles": (C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(C.c_longlong)]),
+    "ecg_compute_mat_elem_tiles": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_longlong, C.c_longlong]),
+    "ecg_pack_tiles": (C.c_int, [_vp, C.c_int, C.c_int, C.c_longlong, C.c_longlong, C.c_void_p]),
+    "ecg_unpack_tiles": (C.c_int, [_vp, C.c_int, C.c_int, C.c_longlong, C.c_longlong, C.c_void_p]),
+    "ecg_adjoint_part_doubles": (C.c_int, [_vp, C.POINTER(C.c_longlong)]),
+    "ecg_adjoint_tiles": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_longlong, C.c_longlong, C.c_void_p]),
+    "ecg_adjoint_finish": (C.c_int, [_vp, C.c_int, C.c_int, C.c_void_p, _dp]),
     "ecg_set_pivot_mode": (C.c_int, [_vp, C.c_int]),
     "ecg_set_wait_limit": (C.c_int, [_vp, C.c_int]),
     "ecg_io_bytes": (C.c_int, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),

@@ -358,6 +358,39 @@ class Context:
         _check(self.lib.ecg_timer_stop(self.h, C.byref(ms)), "ecg_timer_stop")
         return ms.value
 
+    # -- pair tiles split over ranks (see ecg_pair_tiles in ecg_abi.h) ------
+    def pair_tiles(self, nmin, nmax):
+        n = C.c_longlong()
+        _check(self.lib.ecg_pair_tiles(self.h, int(nmin), int(nmax), C.byref(n)), "ecg_pair_tiles")
+        return n.value
+
+    def compute_mat_elem_tiles(self, nmin, nmax, approx_energy, first, count):
+        _check(self.lib.ecg_compute_mat_elem_tiles(self.h, int(nmin), int(nmax), float(approx_energy), int(first),
+                                                   int(count)), "ecg_compute_mat_elem_tiles")
+
+    def pack_tiles(self, nmin, nmax, first, count, ptr):
+        _check(self.lib.ecg_pack_tiles(self.h, int(nmin), int(nmax), int(first), int(count), C.c_void_p(int(ptr))),
+               "ecg_pack_tiles")
+
+    def unpack_tiles(self, nmin, nmax, first, count, ptr):
+        _check(self.lib.ecg_unpack_tiles(self.h, int(nmin), int(nmax), int(first), int(count),
+                                         C.c_void_p(int(ptr))), "ecg_unpack_tiles")
+
+    def adjoint_part_doubles(self):
+        n = C.c_longlong()
+        _check(self.lib.ecg_adjoint_part_doubles(self.h, C.byref(n)), "ecg_adjoint_part_doubles")
+        return n.value
+
+    def adjoint_tiles(self, nfru, nfa, energy, first, count, ptr):
+        _check(self.lib.ecg_adjoint_tiles(self.h, int(nfru), int(nfa), float(energy), int(first), int(count),
+                                          C.c_void_p(int(ptr))), "ecg_adjoint_tiles")
+
+    def adjoint_finish(self, nfru, nfa, ptr):
+        g = np.zeros((nfa - nfru) * self.npt)
+        _check(self.lib.ecg_adjoint_finish(self.h, int(nfru), int(nfa), C.c_void_p(int(ptr)), dptr(g)),
+               "ecg_adjoint_finish")
+        return g
+
     def set_pivot_mode(self, mode):
         """LDL^H pivots: 0 real (default), 1 complex as the reference."""
         _check(self.lib.ecg_set_pivot_mode(self.h, int(mode)), "ecg_set_pivot_mode")

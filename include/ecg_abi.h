@@ -256,6 +256,47 @@ int ecg_sync(ecg_ctx* ctx);
  * records a second one, waits for it and returns the elapsed ms. */
 int ecg_timer_start(ecg_ctx* ctx);
 int ecg_timer_stop(ecg_ctx* ctx, double* ms);
+/* One evaluation's pair work split over several GPUs (one context per GPU,
+ * one process per GPU).  The reference deals its (pair, term) units to MPI
+ * ranks and sums the H, S buffers and the gradient with MPI_ALLREDUCE
+ * (src/matform.f90:170-213, src/workproc.f90:2129,2148); here each rank
+ * takes a contiguous range of the 32 x 32 pair tiles of the lower
+ * triangle, in the order the pair kernels walk them (ecg_pair_tiles gives
+ * their number for rows nmin..nmax):
+ *   ecg_compute_mat_elem_tiles  ComputeMatElem(nmin, nmax) for the range's
+ *                               pairs plus every diagonal pair (StoreHS
+ *                               needs all of diagS), into Glob_H / Glob_S;
+ *   ecg_pack_tiles              the range's stored entries into packed_dev
+ *                               (per tile 2 x 32 x 32 complex: H, then S);
+ *   ecg_unpack_tiles            another rank's packed tiles into Glob_H,
+ *                               Glob_S ('I' storage: S's upper mirror too).
+ * After the exchange every rank holds the whole H and S, bit for bit what
+ * ecg_compute_mat_elem writes, and runs the solve itself (ecg_energy_ia
+ * with mat_elem_needed 0 and SpecifNorm 0).  Then
+ *   ecg_adjoint_tiles           the fused adjoint pass of
+ *                               ecg_energy_ib_adjoint over the range's
+ *                               tiles of rows nfru+1..nfa (the tile list
+ *                               of ecg_pair_tiles(nfru+1, nfa)) with
+ *                               energy E and the eigenvector in
+ *                               Glob_LastEigvector; part_dev receives
+ *                               count x ecg_adjoint_part_doubles values;
+ *   ecg_adjoint_finish          the gradient from the partials of all
+ *                               tiles in list order (the ranks' ranges
+ *                               concatenated): bit for bit that of
+ *                               ecg_energy_ib_adjoint; grad_host as there.
+ * Device buffers are the caller's, on the context's device; work is
+ * ordered on the context's stream (ecg_sync before another stream or a
+ * collective reads them). */
+int ecg_pair_tiles(ecg_ctx* ctx, int nmin, int nmax, long long* ntiles);
+int ecg_compute_mat_elem_tiles(ecg_ctx* ctx, int nmin, int nmax, double approx_energy, long long first,
+                               long long count);
+int ecg_pack_tiles(ecg_ctx* ctx, int nmin, int nmax, long long first, long long count, void* packed_dev);
+int ecg_unpack_tiles(ecg_ctx* ctx, int nmin, int nmax, long long first, long long count, const void* packed_dev);
+int ecg_adjoint_part_doubles(ecg_ctx* ctx, long long* per_tile);
+int ecg_adjoint_tiles(ecg_ctx* ctx, int nfru, int nfa, double energy, long long first, long long count,
+                      void* part_dev);
+int ecg_adjoint_finish(ecg_ctx* ctx, int nfru, int nfa, const void* part_dev, double* grad_host);
+
 /* Pivots of the context's LDL^H factorisations (GHEPIIS, the candidates'
  * bordered step, the 'G' path): mode 0 (default) keeps them real, dropping
  * the rounding-level imaginary part that the complex arithmetic of
