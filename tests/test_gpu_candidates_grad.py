@@ -85,6 +85,9 @@ def test_candidate_gradient_finite_differences():
     assert np.all(errp == 0)
     fd = (Ep[:npt] - Ep[npt:]) / (2 * h)
     gmax = np.max(np.abs(g[j]))
+    # truncation and the energy's rounding over the step (64 eps |E| / h)
+    bound = 1e-6 * gmax + 1e-5 * np.abs(g[j]) + 64 * np.finfo(np.float64).eps * abs(E[j]) / h
     print("analytic", g[j])
     print("fd      ", fd)
-    assert np.all(np.abs(fd - g[j]) <= 1e-6 * gmax + 1e-5 * np.abs(g[j]))
+    print("|fd - analytic| / bound", np.abs(fd - g[j]) / bound)
+    assert np.all(np.abs(fd - g[j]) <= bound)
