@@ -65,8 +65,7 @@ def parse():
     ap.add_argument("--lam", type=float, default=None,
                     help="use this lambda~ instead of the stored one or a search (profiling runs)")
     ap.add_argument("--ref-max-iter", type=int, default=None,
-                    help="MaxIter of the reference arm's GHEPIIS (default: the GPU arm's measured iteration "
-                         "count stored beside lambda~, else 20)")
+                    help="MaxIter of the reference arm's GHEPIIS (default 20, the reference's)")
     return ap.parse_args()
 
 
@@ -714,10 +713,9 @@ def cpu_expc(sysm, params, terms, Kp=300):
 def run_reference(args, dist):
     """The reference arm: the oracle's EnergyIB on the host cores, one full,
     unscaled evaluation per step, on the GPU arm's workload (same basis,
-    lambda~, perturbed parameter sets and warm starts, Tol; MaxIter set to
-    the GPU arm's iteration count, because the oracle's complex pivots leave
-    a residual floor near 2e-12 at this size where the GPU's real pivots
-    converge)."""
+    lambda~, perturbed parameter sets and warm starts, Tol 1e-12 and
+    MaxIter 20 as the reference's inputs set them; --ref-max-iter caps the
+    iterations instead)."""
     if dist.rank != 0:
         return None
     K = args.K or 4000
@@ -729,7 +727,7 @@ def run_reference(args, dist):
         lam = fx["lambda_tilde"]
     else:
         lam = e_floor
-    mi = args.ref_max_iter or (fx or {}).get("gpu_invit_iters") or 20
+    mi = args.ref_max_iter or 20
     sets = perturbed_sets(params, 0)
     t0 = time.perf_counter()
     cb = cpu_sample(sysm, sets, lam, K, args.tol, int(mi), warmup=args.warmup, steps=args.steps)
