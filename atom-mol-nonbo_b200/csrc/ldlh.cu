@@ -9,7 +9,7 @@
 // The factorisation is right-looking over 64-row panels and runs entirely
 // in the upper triangle, which holds the working Schur complement W(r,c),
 // r < c; the working diagonal lives in dw.  Per panel p = [p0,p1):
-//   k_ldl_diag    eliminate the 64 x 64 diagonal block in registers,
+//   k_ldl_diag    eliminate the 64 x 64 diagonal block in shared memory,
 //                 producing U (= L^H) and invD;
 //   k_ldl_trsm    Wun(p, c) by substitution with U_pp, U(p, c) = invD Wun;
 //   k_ldl_bulk    W(r, c) -= sum_q conj(U(q,r)) Wun(q,c), r <= c beyond p
@@ -65,6 +65,26 @@ __global__ void __launch_bounds__(256) k_ldl_mirror(cd* __restrict__ A, int ld, 
     }
 }
 
+// Diagonal block elimination, blocked by 8-row sub-panels.  The working
+// 64 x 64 upper triangle W(r, c), r <= c (diagonal from dw), sits in shared
+// memory.  Per sub-panel (rows s0..s0+7):
+//   (a) one thread eliminates the 8 x 8 diagonal sub-block in its
+//       registers;
+//   (b) one thread per column c beyond the sub-block forms the unscaled
+//       rows Wun(q, c) = W(q, c) - sum_{q' < q} conj(U(q', q)) Wun(q', c)
+//       by substitution and U(q, c) = invD_q Wun(q, c);
+//   (c) the eight warps apply the rank-8 update W(r, c) -= sum_q
+//       conj(U(q, r)) Wun(q, c) to the rows and columns beyond the
+//       sub-panel on the FP64 tensor cores.
+// Three barriers per sub-panel.  The recurrence and the pivot follow
+// src/linalg.f90:359-391: W(q, q) accumulated this way is the reference's
+// pivot conj(x) (M(q, q) is real), zero test included.  CPLX = false
+// (default): the pivot's imaginary part, rounding noise of the updates, is
+// dropped (kept, it sets a floor of 1e-13..1e-12 under GHEPIIS's residual
+// NormOfDiff); true: the complex pivot is kept as the reference keeps it.
+// (A register-resident rank-one form with one barrier per pivot measured
+// slower, 61 against 32 us per 64 x 64 block: 64 dependent pivot steps of
+// FP64 FMA work on eight warps.)
 // one m8n8k4 FP64 tensor-core product, D = A B + C (C = D in place)
 __device__ __forceinline__ void mma_f64(double& c0, double& c1, double a, double b)
 {
@@ -74,116 +94,169 @@ __device__ __forceinline__ void mma_f64(double& c0, double& c1, double a, double
 }
 
 constexpr int DG_LD = LDL_NB + 1;
+constexpr int DG_SUB = 8;
+constexpr size_t DG_SMEM = (size_t)(LDL_NB * DG_LD + DG_SUB * LDL_NB) * sizeof(double2);
 
-// Diagonal block elimination: the working 64 x 64 upper triangle W(r, c),
-// r <= c (diagonal from dw), is held in registers, element (r, c) by lane
-// r mod 32 of warp c mod 8 (two rows and eight columns per thread, so the
-// loads and stores of a warp are whole column segments).  Per pivot q the
-// eight threads holding row q publish it to shared memory; after one
-// barrier every thread reads the pivot d = W(q, q) and applies the rank-one
-// update W(r, c) -= conj(U(q, r)) Wun(q, c), U(q, r) = Wun(q, r)/d, to its
-// elements with q < r <= c; the row-q holders scale their row to U(q, c).
-// Column groups beyond q are tested per warp, the rows below 32 per block,
-// so finished parts cost no issue slots.  The recurrence follows
-// src/linalg.f90:359-391: W(q, q) accumulated this way is the reference's
-// pivot conj(x) (M(q, q) is real), zero test included; only the summation
-// order differs from the reference's row-by-row dot products.
-// CPLX = false (default): the pivot's imaginary part, rounding noise of
-// the updates, is dropped (kept, it sets a floor of 1e-13..1e-12 under
-// GHEPIIS's residual NormOfDiff); true: the complex pivot is kept, as the
-// reference keeps it.
 template <bool CPLX>
 __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, int p0, int p1, cd* __restrict__ dw,
                                                    cd* __restrict__ invD, int* __restrict__ status)
 {
-    __shared__ double2 rb[2][LDL_NB];
+    extern __shared__ double2 dsm[];
+    double2* Ws = dsm;                   // Ws[r * DG_LD + c], r <= c
+    double2* Wu = dsm + LDL_NB * DG_LD;  // Wu[q * LDL_NB + c]: unscaled rows of the sub-panel
+    __shared__ double2 sid[DG_SUB];      // invD of the sub-panel rows
     const int b = p1 - p0;
-    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
-    double wr[2][8], wi[2][8];
-#pragma unroll
-    for (int j = 0; j < 2; j++)
-#pragma unroll
-        for (int a = 0; a < 8; a++) {
-            const int r = lane + 32 * j, c = wp + 8 * a;
-            cd v = cd{0.0, 0.0};
-            if (c < b && r <= c) v = (r == c) ? dw[p0 + r] : A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld];
-            wr[j][a] = v.x;
-            wi[j][a] = v.y;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
+        const int r = e & 63, c = e >> 6;
+        double2 v = make_double2(0.0, 0.0);
+        if (r < b && c < b) {
+            if (r < c) {
+                const cd a = A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld];
+                v = make_double2(a.x, a.y);
+            } else if (r == c) {
+                const cd a = dw[p0 + r];
+                v = make_double2(a.x, a.y);
+            }
         }
-    for (int q = 0; q < b; q++) {
-        const int buf = q & 1, jq = q >> 5;
-        if (lane == (q & 31)) {
+        Ws[r * DG_LD + c] = v;
+    }
+    __syncthreads();
+    for (int s0 = 0; s0 < b; s0 += DG_SUB) {
+        const int nq = min(DG_SUB, b - s0);
+        // (a) 8 x 8 diagonal sub-block, in the registers of one thread: no
+        // shuffles, so a pivot step costs one reciprocal and three dependent
+        // FP64 operations
+        if (tid == 0) {
+            cd a[DG_SUB][DG_SUB];
 #pragma unroll
-            for (int j = 0; j < 2; j++)
-                if (j == jq) {
+            for (int i = 0; i < DG_SUB; i++)
 #pragma unroll
-                    for (int a = 0; a < 8; a++) rb[buf][wp + 8 * a] = make_double2(wr[j][a], wi[j][a]);
+                for (int j = i; j < DG_SUB; j++) {
+                    const double2 v = (j < nq) ? Ws[(s0 + i) * DG_LD + s0 + j] : make_double2(0.0, 0.0);
+                    a[i][j] = cd{v.x, v.y};
                 }
+#pragma unroll
+            for (int q = 0; q < DG_SUB; q++) {
+                if (q < nq) {
+                    // pivot d = W(q, q) (the reference's conj(x), M(q, q) real);
+                    // real: its rounding-level imaginary part dropped
+                    const double dr = a[q][q].x, di = CPLX ? a[q][q].y : 0.0;
+                    const bool zero = (dr == 0.0 && di == 0.0);
+                    double id, idi = 0.0;  // 1 / d
+                    if (CPLX) {
+                        const double m = zero ? 0.0 : __drcp_rn(fma(dr, dr, di * di));
+                        id = dr * m;
+                        idi = -di * m;
+                    } else {
+                        id = zero ? 0.0 : __drcp_rn(dr);
+                    }
+                    sid[q] = make_double2(id, idi);
+                    invD[p0 + s0 + q] = cd{id, idi};
+                    if (zero) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + s0 + q + 1);
+                    cd u[DG_SUB];
+#pragma unroll
+                    for (int j = q + 1; j < DG_SUB; j++)
+                        u[j] = CPLX ? cmul(a[q][j], cd{id, idi}) : cd{a[q][j].x * id, a[q][j].y * id};  // U(q, j)
+#pragma unroll
+                    for (int i = q + 1; i < DG_SUB; i++)
+#pragma unroll
+                        for (int j = i; j < DG_SUB; j++) a[i][j] = cfms(conj(u[i]), a[q][j], a[i][j]);
+#pragma unroll
+                    for (int j = q + 1; j < DG_SUB; j++) a[q][j] = u[j];
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < DG_SUB; i++)
+#pragma unroll
+                for (int j = i + 1; j < DG_SUB; j++)
+                    if (j < nq) Ws[(s0 + i) * DG_LD + s0 + j] = make_double2(a[i][j].x, a[i][j].y);
         }
         __syncthreads();
-        const double2 dq = rb[buf][q];
-        double inv, invi = 0.0;  // 1 / d
-        bool zero;
-        if (CPLX) {
-            zero = (dq.x == 0.0 && dq.y == 0.0);
-            const double m = zero ? 0.0 : __drcp_rn(fma(dq.x, dq.x, dq.y * dq.y));
-            inv = dq.x * m;
-            invi = -dq.y * m;
-        } else {
-            zero = (dq.x == 0.0);
-            inv = zero ? 0.0 : __drcp_rn(dq.x);
-        }
-        if (threadIdx.x == 0) {
-            invD[p0 + q] = cd{inv, invi};
-            if (zero) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + q + 1);
-        }
-        double ur[2], ui[2];
+        // (b) sub-panel rows beyond the sub-block, one thread per column
+        const int t0 = s0 + DG_SUB;
+        if (t0 < b && tid < b - t0) {
+            const int c = t0 + tid;
+            cd wun[DG_SUB];
 #pragma unroll
-        for (int j = 0; j < 2; j++) {
-            const double2 u = rb[buf][lane + 32 * j];  // conj(U(q, r)) = conj(Wun(q, r) / d)
-            if (CPLX) {
-                ur[j] = fma(u.x, inv, -u.y * invi);
-                ui[j] = -fma(u.x, invi, u.y * inv);
-            } else {
-                ur[j] = u.x * inv;
-                ui[j] = -u.y * inv;
-            }
-        }
+            for (int q = 0; q < DG_SUB; q++) {
+                if (q < nq) {
+                    const double2 w = Ws[(s0 + q) * DG_LD + c];
+                    cd v = cd{w.x, w.y};
 #pragma unroll
-        for (int a = 0; a < 8; a++) {
-            const int c = wp + 8 * a;
-            if (c > q) {  // warp-uniform
-                const double2 v = rb[buf][c];
-#pragma unroll
-                for (int j = 0; j < 2; j++) {
-                    const int r = lane + 32 * j;
-                    if (j == 0 && q >= 32) continue;  // block-uniform: rows below 32 are finished
-                    if (r > q && r <= c) {
-                        wr[j][a] = fma(-ur[j], v.x, fma(ui[j], v.y, wr[j][a]));
-                        wi[j][a] = fma(-ur[j], v.y, fma(-ui[j], v.x, wi[j][a]));
-                    } else if (r == q) {
-                        if (CPLX) {
-                            const double x = wr[j][a], y = wi[j][a];
-                            wr[j][a] = fma(x, inv, -y * invi);
-                            wi[j][a] = fma(x, invi, y * inv);
-                        } else {
-                            wr[j][a] *= inv;
-                            wi[j][a] *= inv;
-                        }
+                    for (int q2 = 0; q2 < q; q2++) {
+                        const double2 u = Ws[(s0 + q2) * DG_LD + s0 + q];  // U(q2, q)
+                        v = cfms(cd{u.x, -u.y}, wun[q2], v);
                     }
+                    wun[q] = v;
+                    Wu[q * LDL_NB + c] = make_double2(v.x, v.y);
+                    const double2 id = sid[q];
+                    const cd uq = CPLX ? cmul(v, cd{id.x, id.y}) : cd{v.x * id.x, v.y * id.x};
+                    Ws[(s0 + q) * DG_LD + c] = make_double2(uq.x, uq.y);
+                } else {
+                    wun[q] = cd{0.0, 0.0};
                 }
             }
         }
-    }
+        __syncthreads();
+        // (c) rank-8 update of the rows and columns beyond the sub-panel on
+        // the FP64 tensor cores: 8 x 8 output tiles of the upper triangle
+        // (tile row <= tile column) spread over the eight warps; per tile
+        // and k-step of 4, four m8n8k4 products with the conjugate and the
+        // minus sign folded into the U fragment, accumulated onto W.
+        if (t0 < b) {
+            const int lane = tid & 31, wp = tid >> 5;
+            const int g = lane >> 2, t4 = lane & 3;
+            const int T = (b - t0 + 7) >> 3;
+            const int ntiles = T * (T + 1) / 2;
+            for (int tile = wp; tile < ntiles; tile += 8) {
+                int R = 0, rem = tile;
+                while (rem >= T - R) {
+                    rem -= T - R;
+                    R++;
+                }
+                const int Cc = R + rem;
+                const int r = t0 + 8 * R + g;         // fragment row (C and U)
+                const int cg = t0 + 8 * Cc + g;       // fragment column of Wun
+                const int ca = t0 + 8 * Cc + 2 * t4;  // C columns ca, ca + 1
+                double accr[2], acci[2];
 #pragma unroll
-    for (int j = 0; j < 2; j++)
+                for (int e = 0; e < 2; e++) {
+                    const int c = ca + e;
+                    double2 w = make_double2(0.0, 0.0);
+                    if (r < b && c < b && r <= c) w = Ws[r * DG_LD + c];
+                    accr[e] = w.x;
+                    acci[e] = w.y;
+                }
 #pragma unroll
-        for (int a = 0; a < 8; a++) {
-            const int r = lane + 32 * j, c = wp + 8 * a;
-            if (c < b && r < c) A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld] = cd{wr[j][a], wi[j][a]};
+                for (int k0 = 0; k0 < DG_SUB; k0 += 4) {
+                    const int q = k0 + t4;
+                    double2 u = make_double2(0.0, 0.0), v = make_double2(0.0, 0.0);
+                    if (q < nq && r < b) u = Ws[(s0 + q) * DG_LD + r];  // U(q, r)
+                    if (q < nq && cg < b) v = Wu[q * LDL_NB + cg];      // Wun(q, c)
+                    // W -= conj(U) Wun: Re -= Ur Vr + Ui Vi, Im -= Ur Vi - Ui Vr
+                    mma_f64(accr[0], accr[1], -u.x, v.x);
+                    mma_f64(accr[0], accr[1], -u.y, v.y);
+                    mma_f64(acci[0], acci[1], -u.x, v.y);
+                    mma_f64(acci[0], acci[1], u.y, v.x);
+                }
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int c = ca + e;
+                    if (r < b && c < b && r <= c) Ws[r * DG_LD + c] = make_double2(accr[e], acci[e]);
+                }
+            }
         }
+        __syncthreads();
+    }
+    for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
+        const int r = e & 63, c = e >> 6;
+        if (r < c && c < b) {
+            const double2 v = Ws[r * DG_LD + c];
+            A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld] = cd{v.x, v.y};
+        }
+    }
 }
-
 // Inverse of the unit lower diagonal block L_pp = U_pp^H of every panel in
 // [first, nb) (one CTA per panel, all independent): Gaussian elimination of
 // L applied to the identity, X(r,s) -= L(r,q) X(q,s).  Row r of X lands in
@@ -453,9 +526,9 @@ static void enqueue_factor(Ctx& c, int m0, int n, const std::vector<int>& starts
     };
     auto diag = [&](int p0, int p1) {
         if (c.pivot_mode)
-            k_ldl_diag<true><<<1, 256, 0, c.stream>>>(c.F, c.ld, p0, p1, c.dw, c.invD, c.status);
+            k_ldl_diag<true><<<1, 256, DG_SMEM, c.stream>>>(c.F, c.ld, p0, p1, c.dw, c.invD, c.status);
         else
-            k_ldl_diag<false><<<1, 256, 0, c.stream>>>(c.F, c.ld, p0, p1, c.dw, c.invD, c.status);
+            k_ldl_diag<false><<<1, 256, DG_SMEM, c.stream>>>(c.F, c.ld, p0, p1, c.dw, c.invD, c.status);
         c.launches++;
     };
     if (n > m0) {
@@ -535,6 +608,8 @@ int ldlh_factor(Ctx& c, int m0, int n)
     const size_t sm1 = LDL_NB * DG_LD * sizeof(double2);
     if (!g_ldl_attr) {
         cudaFuncSetAttribute(k_ldl_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+        cudaFuncSetAttribute(k_ldl_diag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DG_SMEM);
+        cudaFuncSetAttribute(k_ldl_diag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DG_SMEM);
         cudaFuncSetAttribute(k_ldl_linv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * sm1));
         cudaFuncSetAttribute(k_ldl_bulk<32, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem<32>());
         cudaFuncSetAttribute(k_ldl_bulk<16, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem<16>());
