@@ -78,7 +78,7 @@ void free_ctx(Ctx& c)
     if (c.stream) {
         for (int i = 0; i < 16; i++) cudaEventDestroy(c.ev[i]);
         for (int i = 0; i < 2; i++) cudaEventDestroy(c.tev[i]);
-        for (int i = 0; i < 2; i++) cudaEventDestroy(c.lev[i]);
+        for (int i = 0; i < 3; i++) cudaEventDestroy(c.lev[i]);
         if (c.side) cudaStreamDestroy(c.side);
         cudaStreamDestroy(c.stream);
     }
@@ -472,7 +472,7 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
     }
     for (int i = 0; i < 16; i++) cudaEventCreate(&c.ev[i]);
     for (int i = 0; i < 2; i++) cudaEventCreate(&c.tev[i]);
-    for (int i = 0; i < 2; i++) cudaEventCreateWithFlags(&c.lev[i], cudaEventDisableTiming);
+    for (int i = 0; i < 3; i++) cudaEventCreateWithFlags(&c.lev[i], cudaEventDisableTiming);
     if (cudaStreamCreateWithPriority(&c.side, cudaStreamNonBlocking, prio_lo) != cudaSuccess) {
         cudaGetLastError();
         free_ctx(c);

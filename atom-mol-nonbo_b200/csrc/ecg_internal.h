@@ -99,7 +99,7 @@ struct Ctx {
     SysParams sp{};
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;   // second stream of the LDL^H lookahead
-    cudaEvent_t lev[2];            // LDL^H lookahead events
+    cudaEvent_t lev[3];            // LDL^H lookahead events
 
     // Glob_* state, device resident
     double* params = nullptr;   // npt x ld, column-major (Glob_NonlinParam)
