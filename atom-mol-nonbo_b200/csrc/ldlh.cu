@@ -76,7 +76,8 @@ __global__ void __launch_bounds__(256) k_ldl_mirror(cd* __restrict__ A, int ld, 
 //   (c) the eight warps apply the rank-8 update W(r, c) -= sum_q
 //       conj(U(q, r)) Wun(q, c) to the rows and columns beyond the
 //       sub-panel on the FP64 tensor cores.
-// Three barriers per sub-panel.  The recurrence and the pivot follow
+// Two barriers per sub-panel: the elimination (a) of the next sub-panel
+// runs beside the update (c) of this one.  The recurrence and the pivot follow
 // src/linalg.f90:359-391: W(q, q) accumulated this way is the reference's
 // pivot conj(x) (M(q, q) is real), zero test included.  CPLX = false
 // (default): the pivot's imaginary part, rounding noise of the updates, is
@@ -122,57 +123,60 @@ __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, in
         Ws[r * DG_LD + c] = v;
     }
     __syncthreads();
-    for (int s0 = 0; s0 < b; s0 += DG_SUB) {
+    // (a) for sub-panel s0: the 8 x 8 diagonal sub-block, in the registers
+    // of one thread (no shuffles, so a pivot step costs one reciprocal and
+    // three dependent FP64 operations)
+    auto eliminate = [&](int s0) {
         const int nq = min(DG_SUB, b - s0);
-        // (a) 8 x 8 diagonal sub-block, in the registers of one thread: no
-        // shuffles, so a pivot step costs one reciprocal and three dependent
-        // FP64 operations
-        if (tid == 0) {
-            cd a[DG_SUB][DG_SUB];
+        cd a[DG_SUB][DG_SUB];
 #pragma unroll
-            for (int i = 0; i < DG_SUB; i++)
+        for (int i = 0; i < DG_SUB; i++)
 #pragma unroll
-                for (int j = i; j < DG_SUB; j++) {
-                    const double2 v = (j < nq) ? Ws[(s0 + i) * DG_LD + s0 + j] : make_double2(0.0, 0.0);
-                    a[i][j] = cd{v.x, v.y};
-                }
-#pragma unroll
-            for (int q = 0; q < DG_SUB; q++) {
-                if (q < nq) {
-                    // pivot d = W(q, q) (the reference's conj(x), M(q, q) real);
-                    // real: its rounding-level imaginary part dropped
-                    const double dr = a[q][q].x, di = CPLX ? a[q][q].y : 0.0;
-                    const bool zero = (dr == 0.0 && di == 0.0);
-                    double id, idi = 0.0;  // 1 / d
-                    if (CPLX) {
-                        const double m = zero ? 0.0 : __drcp_rn(fma(dr, dr, di * di));
-                        id = dr * m;
-                        idi = -di * m;
-                    } else {
-                        id = zero ? 0.0 : __drcp_rn(dr);
-                    }
-                    sid[q] = make_double2(id, idi);
-                    invD[p0 + s0 + q] = cd{id, idi};
-                    if (zero) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + s0 + q + 1);
-                    cd u[DG_SUB];
-#pragma unroll
-                    for (int j = q + 1; j < DG_SUB; j++)
-                        u[j] = CPLX ? cmul(a[q][j], cd{id, idi}) : cd{a[q][j].x * id, a[q][j].y * id};  // U(q, j)
-#pragma unroll
-                    for (int i = q + 1; i < DG_SUB; i++)
-#pragma unroll
-                        for (int j = i; j < DG_SUB; j++) a[i][j] = cfms(conj(u[i]), a[q][j], a[i][j]);
-#pragma unroll
-                    for (int j = q + 1; j < DG_SUB; j++) a[q][j] = u[j];
-                }
+            for (int j = i; j < DG_SUB; j++) {
+                const double2 v = (j < nq) ? Ws[(s0 + i) * DG_LD + s0 + j] : make_double2(0.0, 0.0);
+                a[i][j] = cd{v.x, v.y};
             }
 #pragma unroll
-            for (int i = 0; i < DG_SUB; i++)
+        for (int q = 0; q < DG_SUB; q++) {
+            if (q < nq) {
+                // pivot d = W(q, q) (the reference's conj(x), M(q, q) real);
+                // real: its rounding-level imaginary part dropped
+                const double dr = a[q][q].x, di = CPLX ? a[q][q].y : 0.0;
+                const bool zero = (dr == 0.0 && di == 0.0);
+                double id, idi = 0.0;  // 1 / d
+                if (CPLX) {
+                    const double m = zero ? 0.0 : __drcp_rn(fma(dr, dr, di * di));
+                    id = dr * m;
+                    idi = -di * m;
+                } else {
+                    id = zero ? 0.0 : __drcp_rn(dr);
+                }
+                sid[q] = make_double2(id, idi);
+                invD[p0 + s0 + q] = cd{id, idi};
+                if (zero) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + s0 + q + 1);
+                cd u[DG_SUB];
 #pragma unroll
-                for (int j = i + 1; j < DG_SUB; j++)
-                    if (j < nq) Ws[(s0 + i) * DG_LD + s0 + j] = make_double2(a[i][j].x, a[i][j].y);
+                for (int j = q + 1; j < DG_SUB; j++)
+                    u[j] = CPLX ? cmul(a[q][j], cd{id, idi}) : cd{a[q][j].x * id, a[q][j].y * id};  // U(q, j)
+#pragma unroll
+                for (int i = q + 1; i < DG_SUB; i++)
+#pragma unroll
+                    for (int j = i; j < DG_SUB; j++) a[i][j] = cfms(conj(u[i]), a[q][j], a[i][j]);
+#pragma unroll
+                for (int j = q + 1; j < DG_SUB; j++) a[q][j] = u[j];
+            }
         }
-        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < DG_SUB; i++)
+#pragma unroll
+            for (int j = i + 1; j < DG_SUB; j++)
+                if (j < nq) Ws[(s0 + i) * DG_LD + s0 + j] = make_double2(a[i][j].x, a[i][j].y);
+    };
+    if (tid == 0) eliminate(0);
+    __syncthreads();
+    const int lane = tid & 31, wp = tid >> 5;
+    for (int s0 = 0; s0 < b; s0 += DG_SUB) {
+        const int nq = min(DG_SUB, b - s0);
         // (b) sub-panel rows beyond the sub-block, one thread per column
         const int t0 = s0 + DG_SUB;
         if (t0 < b && tid < b - t0) {
@@ -201,15 +205,17 @@ __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, in
         __syncthreads();
         // (c) rank-8 update of the rows and columns beyond the sub-panel on
         // the FP64 tensor cores: 8 x 8 output tiles of the upper triangle
-        // (tile row <= tile column) spread over the eight warps; per tile
-        // and k-step of 4, four m8n8k4 products with the conjugate and the
-        // minus sign folded into the U fragment, accumulated onto W.
+        // (tile row <= tile column); per tile and k-step of 4, four m8n8k4
+        // products with the conjugate and the minus sign folded into the U
+        // fragment, accumulated onto W.  Warp 0 updates the next diagonal
+        // sub-block (tile 0) and its lane 0 eliminates that sub-block at
+        // once ((a) of the next sub-panel), while warps 1..7 update the
+        // other tiles: the serial elimination overlaps the update.
         if (t0 < b) {
-            const int lane = tid & 31, wp = tid >> 5;
             const int g = lane >> 2, t4 = lane & 3;
             const int T = (b - t0 + 7) >> 3;
             const int ntiles = T * (T + 1) / 2;
-            for (int tile = wp; tile < ntiles; tile += 8) {
+            for (int tile = (wp == 0) ? 0 : wp; tile < ntiles; tile += (wp == 0) ? ntiles : 7) {
                 int R = 0, rem = tile;
                 while (rem >= T - R) {
                     rem -= T - R;
@@ -245,6 +251,10 @@ __global__ void __launch_bounds__(256) k_ldl_diag(cd* __restrict__ A, int ld, in
                     const int c = ca + e;
                     if (r < b && c < b && r <= c) Ws[r * DG_LD + c] = make_double2(accr[e], acci[e]);
                 }
+            }
+            if (wp == 0) {
+                __syncwarp();
+                if (lane == 0) eliminate(t0);
             }
         }
         __syncthreads();
