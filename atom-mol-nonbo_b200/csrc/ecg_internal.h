@@ -17,9 +17,8 @@ constexpr int SOLVE_SPIN_LIMIT = 1 << 22;
 
 // LDL^H block size (rows of one panel).
 constexpr int LDL_NB = 64;
-// Trailing updates apply two panels at once (rank 128); the unscaled panel
-// rows of such a pair are kept with this many rows per column.
-constexpr int LDL_VLD = 2 * LDL_NB;
+// Rows per column of the buffers of unscaled panel rows (one panel).
+constexpr int LDL_VLD = LDL_NB;
 
 // Number of 32 x 32 tiles with row-tile index in [Rlo, Rhi) and column-tile
 // index 0..R (lower triangle including diagonal tiles).
@@ -99,7 +98,7 @@ struct Ctx {
     SysParams sp{};
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;   // second stream of the LDL^H lookahead
-    cudaEvent_t lev[3];            // LDL^H lookahead events
+    cudaEvent_t lev[3];            // LDL^H lookahead events (two in use)
 
     // Glob_* state, device resident
     double* params = nullptr;   // npt x ld, column-major (Glob_NonlinParam)
@@ -135,7 +134,7 @@ struct Ctx {
     // LDL^H workspace
     cd* dw = nullptr;           // working diagonal (ld)
     cd* linv = nullptr;         // ld x LDL_NB: inverse unit-lower diagonal blocks
-    cd* vbuf = nullptr;         // 3 x LDL_VLD x ld: unscaled rows of panel pairs (rotating)
+    cd* vbuf = nullptr;         // 3 x LDL_VLD x ld: unscaled panel rows (rotating)
     int* status = nullptr;      // device status words (see ST_*)
     int* status_h = nullptr;    // pinned host mirror
     double* red = nullptr;      // reduction scratch for the solver (doubles)
