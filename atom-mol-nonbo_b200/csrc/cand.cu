@@ -208,16 +208,18 @@ constexpr size_t TS_SMEM = (size_t)(64 * TS_LDA + CAND_NC * TS_LDB) * sizeof(dou
 
 // G tiles: one CTA per ordered panel pair (p, q), p != q; FWD blocks (p > q)
 // and BWD blocks (p < q) share the array, G(p0+m, q0+n) at Gm[(p0+m) + (q0+n) ld].
-// adj = 1: only the blocks next to the diagonal, into a compact array for
-// the single-vector solves (invit.cu): blockIdx.x = j, blockIdx.y = 0 gives
-// the FWD block (p, q) = (j+1, j), 1 the BWD block (j, j+1), stored
-// row-major at Gm[(2 j + blockIdx.y) 64 x 64 + m 64 + n].
+// adj = 1: only the blocks one and two panels from the diagonal, into a
+// compact array for the single-vector solves (invit.cu): blockIdx.x = j,
+// blockIdx.y = 0, 1, 2, 3 give the FWD block (p, q) = (j+1, j), the BWD
+// block (j, j+1), the FWD block (j+2, j) and the BWD block (j, j+2), stored
+// row-major at Gm[(4 j + blockIdx.y) 64 x 64 + m 64 + n].
 __global__ void __launch_bounds__(256) k_cand_gmat(const cd* __restrict__ H, int ld, const int* __restrict__ bstart,
                                                    int nb, const cd* __restrict__ linv, cd* __restrict__ Gm, int adj)
 {
     extern __shared__ double2 gsm[];
-    const int p = adj ? (int)blockIdx.x + (blockIdx.y == 0 ? 1 : 0) : (int)blockIdx.x;
-    const int q = adj ? (int)blockIdx.x + (blockIdx.y == 0 ? 0 : 1) : (int)blockIdx.y;
+    const int dist = 1 + (int)(blockIdx.y >> 1), bw = (int)(blockIdx.y & 1);
+    const int p = adj ? (int)blockIdx.x + (bw ? 0 : dist) : (int)blockIdx.x;
+    const int q = adj ? (int)blockIdx.x + (bw ? dist : 0) : (int)blockIdx.y;
     if (p == q || p >= nb || q >= nb) return;
     const bool fwd = p > q;
     const int p0 = bstart[p], bp = bstart[p + 1] - p0;
@@ -269,7 +271,7 @@ __global__ void __launch_bounds__(256) k_cand_gmat(const cd* __restrict__ H, int
 #pragma unroll
             for (int e = 0; e < 2; e++) {
                 const int m = wm + mt * 8 + g, n = wn + nt * 8 + 2 * t + e;
-                cd* dst = adj ? Gm + ((size_t)(2 * blockIdx.x + blockIdx.y) * LDL_NB + m) * LDL_NB + n
+                cd* dst = adj ? Gm + ((size_t)(4 * blockIdx.x + blockIdx.y) * LDL_NB + m) * LDL_NB + n
                               : Gm + (size_t)(p0 + m) + (size_t)(q0 + n) * ld;
                 if (adj || (m < bp && n < bq))
                     *reinterpret_cast<double2*>(dst) =
@@ -986,8 +988,9 @@ void cand_free(CandWork& cw)
     cw.solve_grid = sg;
 }
 
-// The blocks next to the diagonal premultiplied by the inverse diagonal
-// blocks, for the single-vector solves: gadj (2 (nb - 1) x 64 x 64).
+// The blocks one and two panels from the diagonal premultiplied by the
+// inverse diagonal blocks, for the single-vector solves: gadj
+// (4 (nb - 1) x 64 x 64; the distance-2 entries of the last j stay unused).
 void launch_adjacent_g(Ctx& c, int nb, const int* bstart_dev, cd* gadj, cudaStream_t st)
 {
     if (nb < 2) return;
@@ -996,7 +999,7 @@ void launch_adjacent_g(Ctx& c, int nb, const int* bstart_dev, cd* gadj, cudaStre
         cudaFuncSetAttribute(k_cand_gmat, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(G_STAGE * sizeof(double2)));
         attr = true;
     }
-    k_cand_gmat<<<dim3(nb - 1, 2), 256, G_STAGE * sizeof(double2), st>>>(c.F, c.ld, bstart_dev, nb, c.linv, gadj, 1);
+    k_cand_gmat<<<dim3(nb - 1, 4), 256, G_STAGE * sizeof(double2), st>>>(c.F, c.ld, bstart_dev, nb, c.linv, gadj, 1);
     c.launches++;
 }
 

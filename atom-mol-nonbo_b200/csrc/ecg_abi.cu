@@ -504,7 +504,7 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
     r |= dalloc(&c.detL, L);
     r |= dalloc(&c.dw, L);
     r |= dalloc(&c.linv, L * LDL_NB);
-    r |= dalloc(&c.gadj, 2 * (L / LDL_NB + 2) * LDL_NB * LDL_NB);
+    r |= dalloc(&c.gadj, 4 * (L / LDL_NB + 2) * LDL_NB * LDL_NB);
     c.gadj_cap = (int)(L / LDL_NB + 2);
     r |= dalloc(&c.vbuf, 3 * L * LDL_VLD);
     r |= dalloc(&c.status, (size_t)ST_COUNT);

@@ -134,7 +134,7 @@ struct Ctx {
     // LDL^H workspace
     cd* dw = nullptr;           // working diagonal (ld)
     cd* linv = nullptr;         // ld x LDL_NB: inverse unit-lower diagonal blocks
-    cd* gadj = nullptr;         // 2 x (panels - 1) x 64 x 64: blocks next to the diagonal times Linv (solves)
+    cd* gadj = nullptr;         // 4 x (panels - 1) x 64 x 64: blocks 1, 2 panels off the diagonal times Linv (solves)
     int gadj_cap = 0;           // panel pairs gadj holds
     cd* vbuf = nullptr;         // 3 x LDL_VLD x ld: unscaled panel rows (rotating)
     int* status = nullptr;      // device status words (see ST_*)

@@ -241,11 +241,11 @@ __device__ __forceinline__ void load_gblock(const cd* __restrict__ gblk, cd (&gk
     for (int kk = 0; kk < 16; kk++) gk[kk] = ld2(gblk + (size_t)r * LDL_NB + 16 * g + kk);
 }
 
-// Forward: y_j = Linv_j (w_j - sum_{a<j-1} U(a, j)^H y_a) - G_j y_{j-1},
-// G_j = Linv_j U(j-1, j)^H (from gadj), z_j = invD_j y_j.  Everything but
-// the last product is done while panel j-1 is still being solved, so a step
-// of the panel chain is one flag hand-off and one 64 x 64 product with a
-// block already in registers.
+// Forward: y_j = Linv_j (w_j - sum_{a<j-2} U(a, j)^H y_a) - G(j, j-2) y_{j-2}
+// - G(j, j-1) y_{j-1}, G(j, a) = Linv_j U(a, j)^H (from gadj), z_j = invD_j
+// y_j.  The sum and its Linv_j product are done while panels j-2 and j-1
+// are still being solved, so a step of the panel chain is one flag
+// hand-off and one 64 x 64 product with a block already in registers.
 __global__ void __launch_bounds__(256, 2) k_fwd_coop(const cd* __restrict__ A, int ld, const int* __restrict__ bstart,
                                                      int nb, const cd* __restrict__ w, cd* __restrict__ y,
                                                      cd* __restrict__ z, const cd* __restrict__ invD,
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(256, 2) k_fwd_coop(const cd* __restrict__ A, i
 #pragma unroll
     for (int m = 0; m < 8; m++) acc[m] = mk(0.0, 0.0);
     bool ok = true;
-    for (int a = 0; a < j - 1; a++) {
+    for (int a = 0; a < j - 2; a++) {
         const int a0 = bstart[a], a1 = bstart[a + 1];
         const int r0 = a0 + lane, r1 = a0 + lane + 32;
         // the factor block U(panel a, panel j) does not depend on panel a's
@@ -322,20 +322,24 @@ __global__ void __launch_bounds__(256, 2) k_fwd_coop(const cd* __restrict__ A, i
         for (int g = 0; g < 4; g++) s = s + mk(red[g * LDL_NB + r].x, red[g * LDL_NB + r].y);
         t[r] = make_double2(s.x, s.y);
     }
-    if (j > 0) {
-        // the chain step: G_j y_{j-1}
+    // the two chain steps: G(j, j-2) y_{j-2}, then G(j, j-1) y_{j-1}, each
+    // block loaded before its panel's flag is awaited
+    for (int d = 2; d >= 1; d--) {
+        if (j - d < 0) continue;
         cd gk[16];
-        load_gblock(gadj + (size_t)(2 * (j - 1)) * LDL_NB * LDL_NB, gk);
-        const int a0 = bstart[j - 1], na = bstart[j] - a0;
-        if (wait_panel(flags, j - 1, epoch, status, abort_word, ok)) chain_matvec(gk, y, a0, na, red);
-        __syncthreads();
+        load_gblock(gadj + (size_t)(4 * (j - d) + 2 * (d - 1)) * LDL_NB * LDL_NB, gk);
+        const int a0 = bstart[j - d], na = bstart[j - d + 1] - a0;
+        if (wait_panel(flags, j - d, epoch, status, abort_word, ok)) chain_matvec(gk, y, a0, na, red + (d - 1) * 4 * LDL_NB);
     }
+    __syncthreads();
     if (threadIdx.x < b) {
         const int r = threadIdx.x;
         cd s = mk(t[r].x, t[r].y);
-        if (j > 0) {
+        for (int d = 2; d >= 1; d--) {
+            if (j - d < 0) continue;
+            const double2* rd = red + (d - 1) * 4 * LDL_NB;
 #pragma unroll
-            for (int g = 0; g < 4; g++) s = s - mk(red[g * LDL_NB + r].x, red[g * LDL_NB + r].y);
+            for (int g = 0; g < 4; g++) s = s - mk(rd[g * LDL_NB + r].x, rd[g * LDL_NB + r].y);
         }
         y[j0 + r] = s;
         z[j0 + r] = cmul(s, ld2(invD + j0 + r));
@@ -345,8 +349,9 @@ __global__ void __launch_bounds__(256, 2) k_fwd_coop(const cd* __restrict__ A, i
     if (threadIdx.x == 0 && ok) st_release(flags + j, epoch);
 }
 
-// Backward: x_j = Linv_j^H (z_j - sum_{c>j+1} U(j, c) x_c) - G_j x_{j+1},
-// G_j = Linv_j^H U(j, j+1) (from gadj); the chain step as in k_fwd_coop.
+// Backward: x_j = Linv_j^H (z_j - sum_{c>j+2} U(j, c) x_c) - G(j, j+2)
+// x_{j+2} - G(j, j+1) x_{j+1}, G(j, c) = Linv_j^H U(j, c) (from gadj); the
+// chain steps as in k_fwd_coop.
 __global__ void __launch_bounds__(256, 2) k_bwd_coop(const cd* __restrict__ A, int ld, const int* __restrict__ bstart,
                                                      int nb, const cd* __restrict__ z, cd* __restrict__ x,
                                                      const cd* __restrict__ linv, const cd* __restrict__ gadj,
@@ -363,7 +368,7 @@ __global__ void __launch_bounds__(256, 2) k_bwd_coop(const cd* __restrict__ A, i
     load_linv(linv, j0, b, Ls);
     cd a0 = mk(0.0, 0.0), a1 = mk(0.0, 0.0);  // rows lane, lane + 32
     bool ok = true;
-    for (int c = nb - 1; c > j + 1; c--) {
+    for (int c = nb - 1; c > j + 2; c--) {
         const int c0 = bstart[c], c1 = bstart[c + 1];
         // U(panel j, panel c) before the wait for panel c's solution
         cd u0[8], u1[8];
@@ -413,20 +418,23 @@ __global__ void __launch_bounds__(256, 2) k_bwd_coop(const cd* __restrict__ A, i
         for (int g = 0; g < 4; g++) s = s + mk(red[g * LDL_NB + r].x, red[g * LDL_NB + r].y);
         t[r] = make_double2(s.x, s.y);
     }
-    if (j + 1 < nb) {
-        // the chain step: G_j x_{j+1}
+    // the two chain steps: G(j, j+2) x_{j+2}, then G(j, j+1) x_{j+1}
+    for (int d = 2; d >= 1; d--) {
+        if (j + d >= nb) continue;
         cd gk[16];
-        load_gblock(gadj + (size_t)(2 * j + 1) * LDL_NB * LDL_NB, gk);
-        const int c0 = bstart[j + 1], ncn = bstart[j + 2] - c0;
-        if (wait_panel(flags, j + 1, epoch, status, abort_word, ok)) chain_matvec(gk, x, c0, ncn, red);
-        __syncthreads();
+        load_gblock(gadj + (size_t)(4 * j + 2 * (d - 1) + 1) * LDL_NB * LDL_NB, gk);
+        const int c0 = bstart[j + d], ncn = bstart[j + d + 1] - c0;
+        if (wait_panel(flags, j + d, epoch, status, abort_word, ok)) chain_matvec(gk, x, c0, ncn, red + (d - 1) * 4 * LDL_NB);
     }
+    __syncthreads();
     if (threadIdx.x < b) {
         const int r = threadIdx.x;
         cd s = mk(t[r].x, t[r].y);
-        if (j + 1 < nb) {
+        for (int d = 2; d >= 1; d--) {
+            if (j + d >= nb) continue;
+            const double2* rd = red + (d - 1) * 4 * LDL_NB;
 #pragma unroll
-            for (int g = 0; g < 4; g++) s = s - mk(red[g * LDL_NB + r].x, red[g * LDL_NB + r].y);
+            for (int g = 0; g < 4; g++) s = s - mk(rd[g * LDL_NB + r].x, rd[g * LDL_NB + r].y);
         }
         x[j0 + r] = s;
         __threadfence();

@@ -633,7 +633,7 @@ int ldlh_factor(Ctx& c, int m0, int n)
         if (c.gadj) cudaFree(c.gadj);
         c.gadj = nullptr;
         c.gadj_cap = 0;
-        if (cudaMalloc((void**)&c.gadj, (size_t)2 * cap * LDL_NB * LDL_NB * sizeof(cd)) != cudaSuccess) {
+        if (cudaMalloc((void**)&c.gadj, (size_t)4 * cap * LDL_NB * LDL_NB * sizeof(cd)) != cudaSuccess) {
             cudaGetLastError();
             c.gadj = nullptr;
             return -3;
