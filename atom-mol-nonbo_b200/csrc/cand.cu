@@ -208,18 +208,11 @@ constexpr size_t TS_SMEM = (size_t)(64 * TS_LDA + CAND_NC * TS_LDB) * sizeof(dou
 
 // G tiles: one CTA per ordered panel pair (p, q), p != q; FWD blocks (p > q)
 // and BWD blocks (p < q) share the array, G(p0+m, q0+n) at Gm[(p0+m) + (q0+n) ld].
-// adj = 1: only the blocks one and two panels from the diagonal, into a
-// compact array for the single-vector solves (invit.cu): blockIdx.x = j,
-// blockIdx.y = 0, 1, 2, 3 give the FWD block (p, q) = (j+1, j), the BWD
-// block (j, j+1), the FWD block (j+2, j) and the BWD block (j, j+2), stored
-// row-major at Gm[(4 j + blockIdx.y) 64 x 64 + m 64 + n].
 __global__ void __launch_bounds__(256) k_cand_gmat(const cd* __restrict__ H, int ld, const int* __restrict__ bstart,
-                                                   int nb, const cd* __restrict__ linv, cd* __restrict__ Gm, int adj)
+                                                   int nb, const cd* __restrict__ linv, cd* __restrict__ Gm)
 {
     extern __shared__ double2 gsm[];
-    const int dist = 1 + (int)(blockIdx.y >> 1), bw = (int)(blockIdx.y & 1);
-    const int p = adj ? (int)blockIdx.x + (bw ? 0 : dist) : (int)blockIdx.x;
-    const int q = adj ? (int)blockIdx.x + (bw ? dist : 0) : (int)blockIdx.y;
+    const int p = blockIdx.x, q = blockIdx.y;
     if (p == q || p >= nb || q >= nb) return;
     const bool fwd = p > q;
     const int p0 = bstart[p], bp = bstart[p + 1] - p0;
@@ -271,11 +264,9 @@ __global__ void __launch_bounds__(256) k_cand_gmat(const cd* __restrict__ H, int
 #pragma unroll
             for (int e = 0; e < 2; e++) {
                 const int m = wm + mt * 8 + g, n = wn + nt * 8 + 2 * t + e;
-                cd* dst = adj ? Gm + ((size_t)(4 * blockIdx.x + blockIdx.y) * LDL_NB + m) * LDL_NB + n
-                              : Gm + (size_t)(p0 + m) + (size_t)(q0 + n) * ld;
-                if (adj || (m < bp && n < bq))
-                    *reinterpret_cast<double2*>(dst) =
-                        (m < bp && n < bq) ? make_double2(acc.r[mt][nt][e], acc.i[mt][nt][e]) : make_double2(0.0, 0.0);
+                if (m < bp && n < bq)
+                    *reinterpret_cast<double2*>(Gm + (size_t)(p0 + m) + (size_t)(q0 + n) * ld) =
+                        make_double2(acc.r[mt][nt][e], acc.i[mt][nt][e]);
             }
 }
 
@@ -988,21 +979,6 @@ void cand_free(CandWork& cw)
     cw.solve_grid = sg;
 }
 
-// The blocks one and two panels from the diagonal premultiplied by the
-// inverse diagonal blocks, for the single-vector solves: gadj
-// (4 (nb - 1) x 64 x 64; the distance-2 entries of the last j stay unused).
-void launch_adjacent_g(Ctx& c, int nb, const int* bstart_dev, cd* gadj, cudaStream_t st)
-{
-    if (nb < 2) return;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_cand_gmat, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(G_STAGE * sizeof(double2)));
-        attr = true;
-    }
-    k_cand_gmat<<<dim3(nb - 1, 4), 256, G_STAGE * sizeof(double2), st>>>(c.F, c.ld, bstart_dev, nb, c.linv, gadj, 1);
-    c.launches++;
-}
-
 // See ecg_eval_candidates / ecg_eval_candidates_grad in ecg_abi.h.  Returns
 // 0 or a negative status; per-candidate ErrorCodes go to errcodes.  With
 // grad (host, npt x count), every candidate's energy gradient with respect
@@ -1067,7 +1043,7 @@ int eval_candidates(Ctx& c, int nbase, int count, const double* cand_host, doubl
     // off-diagonal blocks premultiplied by the inverse diagonal blocks
     if (nb > 1) {
         k_cand_gmat<<<dim3(nb, nb), 256, G_STAGE * sizeof(double2), c.stream>>>(c.F, c.ld, cw.bstart, nb, c.linv,
-                                                                                 cw.Gm, 0);
+                                                                                 cw.Gm);
         c.launches++;
     }
     // bordered factor row: Acol = L0^-1 Mcol, Lcol = invD o Acol, then d_K

@@ -134,8 +134,6 @@ struct Ctx {
     // LDL^H workspace
     cd* dw = nullptr;           // working diagonal (ld)
     cd* linv = nullptr;         // ld x LDL_NB: inverse unit-lower diagonal blocks
-    cd* gadj = nullptr;         // 4 x (panels - 1) x 64 x 64: blocks 1, 2 panels off the diagonal times Linv (solves)
-    int gadj_cap = 0;           // panel pairs gadj holds
     cd* vbuf = nullptr;         // 3 x LDL_VLD x ld: unscaled panel rows (rotating)
     int* status = nullptr;      // device status words (see ST_*)
     int* status_h = nullptr;    // pinned host mirror
@@ -210,7 +208,6 @@ int launch_term_batch(Ctx& c, int count, const double* pk, const double* pl, con
                       cd* hs, cd* dk, cd* dl);
 
 int launch_cand_rows(Ctx& c, CandWork& cw, int nbase, int count, double approx_e, int variant);
-void launch_adjacent_g(Ctx& c, int nb, const int* bstart_dev, cd* gadj, cudaStream_t st);
 // Pair tiles split over ranks: a range of the off-diagonal tile list of
 // rows [r0, r1) (tile_count order), its packing, and the adjoint pass over
 // a range with the gradient from all partials.

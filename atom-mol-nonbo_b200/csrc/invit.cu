@@ -216,42 +216,12 @@ __device__ __forceinline__ void load_linv(const cd* __restrict__ linv, int j0, i
     }
 }
 
-// The last step of a panel's solve, on the chain: s(r) = sum_k G(r, k)
-// v(k) with G the 64 x 64 block (row-major, loaded by the caller before
-// the wait), thread (r = tid & 63, group tid >> 6) taking k = 16 g..16 g+15;
-// the four group sums go to red[g][r].
-__device__ __forceinline__ void chain_matvec(const cd (&gk)[16], const cd* __restrict__ v, int k0, int nk,
-                                             double2* red)
-{
-    const int r = threadIdx.x & 63, g = threadIdx.x >> 6;
-    cd s = mk(0.0, 0.0);
-#pragma unroll
-    for (int kk = 0; kk < 16; kk++) {
-        const int k = 16 * g + kk;
-        const cd vk = (k < nk) ? ldcg2(v + k0 + k) : mk(0.0, 0.0);
-        s = cfma(gk[kk], vk, s);
-    }
-    red[g * LDL_NB + r] = make_double2(s.x, s.y);
-}
-
-__device__ __forceinline__ void load_gblock(const cd* __restrict__ gblk, cd (&gk)[16])
-{
-    const int r = threadIdx.x & 63, g = threadIdx.x >> 6;
-#pragma unroll
-    for (int kk = 0; kk < 16; kk++) gk[kk] = ld2(gblk + (size_t)r * LDL_NB + 16 * g + kk);
-}
-
-// Forward: y_j = Linv_j (w_j - sum_{a<j-2} U(a, j)^H y_a) - G(j, j-2) y_{j-2}
-// - G(j, j-1) y_{j-1}, G(j, a) = Linv_j U(a, j)^H (from gadj), z_j = invD_j
-// y_j.  The sum and its Linv_j product are done while panels j-2 and j-1
-// are still being solved, so a step of the panel chain is one flag
-// hand-off and one 64 x 64 product with a block already in registers.
-__global__ void __launch_bounds__(256, 2) k_fwd_coop(const cd* __restrict__ A, int ld, const int* __restrict__ bstart,
-                                                     int nb, const cd* __restrict__ w, cd* __restrict__ y,
-                                                     cd* __restrict__ z, const cd* __restrict__ invD,
-                                                     const cd* __restrict__ linv, const cd* __restrict__ gadj,
-                                                     unsigned* __restrict__ flags, unsigned epoch,
-                                                     int* __restrict__ status, int* abort_word)
+// Forward: y_j = Linv_j (w_j - sum_{a<j} U(a, j)^H y_a), z_j = invD_j y_j.
+__global__ void __launch_bounds__(256) k_fwd_coop(const cd* __restrict__ A, int ld, const int* __restrict__ bstart,
+                                                  int nb, const cd* __restrict__ w, cd* __restrict__ y,
+                                                  cd* __restrict__ z, const cd* __restrict__ invD,
+                                                  const cd* __restrict__ linv, unsigned* __restrict__ flags,
+                                                  unsigned epoch, int* __restrict__ status, int* abort_word)
 {
     extern __shared__ double2 sm[];
     double2* Ls = sm;                          // Linv_j, [r][q]
@@ -266,7 +236,7 @@ __global__ void __launch_bounds__(256, 2) k_fwd_coop(const cd* __restrict__ A, i
 #pragma unroll
     for (int m = 0; m < 8; m++) acc[m] = mk(0.0, 0.0);
     bool ok = true;
-    for (int a = 0; a < j - 2; a++) {
+    for (int a = 0; a < j; a++) {
         const int a0 = bstart[a], a1 = bstart[a + 1];
         const int r0 = a0 + lane, r1 = a0 + lane + 32;
         // the factor block U(panel a, panel j) does not depend on panel a's
@@ -320,43 +290,19 @@ __global__ void __launch_bounds__(256, 2) k_fwd_coop(const cd* __restrict__ A, i
         cd s = mk(0.0, 0.0);
 #pragma unroll
         for (int g = 0; g < 4; g++) s = s + mk(red[g * LDL_NB + r].x, red[g * LDL_NB + r].y);
-        t[r] = make_double2(s.x, s.y);
-    }
-    // the two chain steps: G(j, j-2) y_{j-2}, then G(j, j-1) y_{j-1}, each
-    // block loaded before its panel's flag is awaited
-    for (int d = 2; d >= 1; d--) {
-        if (j - d < 0) continue;
-        cd gk[16];
-        load_gblock(gadj + (size_t)(4 * (j - d) + 2 * (d - 1)) * LDL_NB * LDL_NB, gk);
-        const int a0 = bstart[j - d], na = bstart[j - d + 1] - a0;
-        if (wait_panel(flags, j - d, epoch, status, abort_word, ok)) chain_matvec(gk, y, a0, na, red + (d - 1) * 4 * LDL_NB);
-    }
-    __syncthreads();
-    if (threadIdx.x < b) {
-        const int r = threadIdx.x;
-        cd s = mk(t[r].x, t[r].y);
-        for (int d = 2; d >= 1; d--) {
-            if (j - d < 0) continue;
-            const double2* rd = red + (d - 1) * 4 * LDL_NB;
-#pragma unroll
-            for (int g = 0; g < 4; g++) s = s - mk(rd[g * LDL_NB + r].x, rd[g * LDL_NB + r].y);
-        }
         y[j0 + r] = s;
         z[j0 + r] = cmul(s, ld2(invD + j0 + r));
         __threadfence();
     }
     __syncthreads();
-    if (threadIdx.x == 0 && ok) st_release(flags + j, epoch);
+    if (threadIdx.x == 0) st_release(flags + j, epoch);
 }
 
-// Backward: x_j = Linv_j^H (z_j - sum_{c>j+2} U(j, c) x_c) - G(j, j+2)
-// x_{j+2} - G(j, j+1) x_{j+1}, G(j, c) = Linv_j^H U(j, c) (from gadj); the
-// chain steps as in k_fwd_coop.
-__global__ void __launch_bounds__(256, 2) k_bwd_coop(const cd* __restrict__ A, int ld, const int* __restrict__ bstart,
-                                                     int nb, const cd* __restrict__ z, cd* __restrict__ x,
-                                                     const cd* __restrict__ linv, const cd* __restrict__ gadj,
-                                                     unsigned* __restrict__ flags, unsigned epoch,
-                                                     int* __restrict__ status, int* abort_word)
+// Backward: x_j = Linv_j^H (z_j - sum_{c>j} U(j, c) x_c).
+__global__ void __launch_bounds__(256) k_bwd_coop(const cd* __restrict__ A, int ld, const int* __restrict__ bstart,
+                                                  int nb, const cd* __restrict__ z, cd* __restrict__ x,
+                                                  const cd* __restrict__ linv, unsigned* __restrict__ flags,
+                                                  unsigned epoch, int* __restrict__ status, int* abort_word)
 {
     extern __shared__ double2 sm[];
     double2* Ls = sm;
@@ -368,7 +314,7 @@ __global__ void __launch_bounds__(256, 2) k_bwd_coop(const cd* __restrict__ A, i
     load_linv(linv, j0, b, Ls);
     cd a0 = mk(0.0, 0.0), a1 = mk(0.0, 0.0);  // rows lane, lane + 32
     bool ok = true;
-    for (int c = nb - 1; c > j + 2; c--) {
+    for (int c = nb - 1; c > j; c--) {
         const int c0 = bstart[c], c1 = bstart[c + 1];
         // U(panel j, panel c) before the wait for panel c's solution
         cd u0[8], u1[8];
@@ -416,31 +362,11 @@ __global__ void __launch_bounds__(256, 2) k_bwd_coop(const cd* __restrict__ A, i
         cd s = mk(0.0, 0.0);
 #pragma unroll
         for (int g = 0; g < 4; g++) s = s + mk(red[g * LDL_NB + r].x, red[g * LDL_NB + r].y);
-        t[r] = make_double2(s.x, s.y);
-    }
-    // the two chain steps: G(j, j+2) x_{j+2}, then G(j, j+1) x_{j+1}
-    for (int d = 2; d >= 1; d--) {
-        if (j + d >= nb) continue;
-        cd gk[16];
-        load_gblock(gadj + (size_t)(4 * j + 2 * (d - 1) + 1) * LDL_NB * LDL_NB, gk);
-        const int c0 = bstart[j + d], ncn = bstart[j + d + 1] - c0;
-        if (wait_panel(flags, j + d, epoch, status, abort_word, ok)) chain_matvec(gk, x, c0, ncn, red + (d - 1) * 4 * LDL_NB);
-    }
-    __syncthreads();
-    if (threadIdx.x < b) {
-        const int r = threadIdx.x;
-        cd s = mk(t[r].x, t[r].y);
-        for (int d = 2; d >= 1; d--) {
-            if (j + d >= nb) continue;
-            const double2* rd = red + (d - 1) * 4 * LDL_NB;
-#pragma unroll
-            for (int g = 0; g < 4; g++) s = s - mk(rd[g * LDL_NB + r].x, rd[g * LDL_NB + r].y);
-        }
         x[j0 + r] = s;
         __threadfence();
     }
     __syncthreads();
-    if (threadIdx.x == 0 && ok) st_release(flags + j, epoch);
+    if (threadIdx.x == 0) st_release(flags + j, epoch);
 }
 
 // Block-wide deterministic sums (1024 threads).
@@ -623,14 +549,13 @@ static int solve_cooperative(Ctx& c, int n)
     const cd* linv = c.linv;
     int ld = c.ld;
     unsigned e1 = ++c.epoch;
-    const cd* gadj = c.gadj;
-    void* a1[] = {(void*)&H, &ld, (void*)&bs, &nb, (void*)&w, &c.yv, &c.zv, (void*)&invD, (void*)&linv, (void*)&gadj,
-                  &c.flags, &e1, &c.status, &abort_word};
+    void* a1[] = {(void*)&H, &ld, (void*)&bs, &nb, (void*)&w, &c.yv, &c.zv, (void*)&invD, (void*)&linv, &c.flags,
+                  &e1, &c.status, &abort_word};
     if (cudaLaunchCooperativeKernel((const void*)k_fwd_coop, nb, 256, a1, sm, c.stream) != cudaSuccess) return -2;
     unsigned e2 = ++c.epoch;
     const cd* zv = c.zv;
-    void* a2[] = {(void*)&H, &ld, (void*)&bs, &nb, (void*)&zv, &c.x, (void*)&linv, (void*)&gadj, &c.flags, &e2,
-                  &c.status, &abort_word};
+    void* a2[] = {(void*)&H, &ld, (void*)&bs, &nb, (void*)&zv, &c.x, (void*)&linv, &c.flags, &e2, &c.status,
+                  &abort_word};
     if (cudaLaunchCooperativeKernel((const void*)k_bwd_coop, nb, 256, a2, sm, c.stream) != cudaSuccess) return -2;
     c.launches += 2;
     return 0;

@@ -589,9 +589,6 @@ static void enqueue_factor(Ctx& c, int m0, int n, const std::vector<int>& starts
         k_ldl_linv<<<nblk - nexist, 256, 2 * sm1, c.stream>>>(c.F, c.ld, c.dblk, nexist, c.linv);
         c.launches++;
     }
-    // the blocks next to the diagonal premultiplied by Linv, for the chain
-    // steps of the triangular solves
-    launch_adjacent_g(c, nblk, c.dblk, c.gadj, c.stream);
 }
 
 // Factorise rows m0..n-1 of M = H - lambda~ S given the factor of rows
@@ -625,24 +622,6 @@ int ldlh_factor(Ctx& c, int m0, int n)
     if (cudaMemcpyAsync(c.dblk, c.bounds_h, (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, c.stream) !=
         cudaSuccess)
         return -2;
-    // the adjacent-block array grows with the panel count (bordered updates
-    // add short panels); the graphs that hold the old pointer are dropped
-    if (nb - 1 > c.gadj_cap) {
-        const int cap = std::max(nb - 1, c.ld / LDL_NB + 2);
-        if (cudaStreamSynchronize(c.stream) != cudaSuccess) return -2;
-        if (c.gadj) cudaFree(c.gadj);
-        c.gadj = nullptr;
-        c.gadj_cap = 0;
-        if (cudaMalloc((void**)&c.gadj, (size_t)4 * cap * LDL_NB * LDL_NB * sizeof(cd)) != cudaSuccess) {
-            cudaGetLastError();
-            c.gadj = nullptr;
-            return -3;
-        }
-        c.gadj_cap = cap;
-        for (auto& e : c.ldl_graphs)
-            if (e.exec) cudaGraphExecDestroy(e.exec);
-        c.ldl_graphs.clear();
-    }
     std::vector<int> key = {m0, n, c.pivot_mode};
     key.insert(key.end(), starts.begin(), starts.begin() + nexist);
     Ctx::LdlGraph* g = nullptr;
