@@ -650,6 +650,20 @@ int ecg_adjoint_finish(ecg_ctx* ctx, int nfru, int nfa, const void* part_dev, do
     return ECG_OK;
 }
 
+int ecg_get_tuning(ecg_ctx* ctx, int* pair_shape, int* adjoint_shape, int* cand_row_shape, double* times_ms)
+{
+    if (!ctx) return ECG_EARG;
+    Ctx& c = ctx->c;
+    if (pair_shape) *pair_shape = c.tune_pair;
+    if (adjoint_shape) *adjoint_shape = c.tune_adj;
+    if (cand_row_shape) *cand_row_shape = c.cand.row_variant;
+    if (times_ms) {
+        for (int v = 0; v < PAIR_SHAPES; v++) times_ms[v] = c.tune_pair_ms[v];
+        for (int v = 0; v < ADJ_SHAPES; v++) times_ms[PAIR_SHAPES + v] = c.tune_adj_ms[v];
+    }
+    return ECG_OK;
+}
+
 int ecg_set_pivot_mode(ecg_ctx* ctx, int mode)
 {
     if (!ctx || mode < 0 || mode > 1) return ECG_EARG;

@@ -30,6 +30,10 @@ inline long long tile_count(int Rlo, int Rhi)
 
 // Number of k_cand_row tile shapes the autotuner chooses from.
 constexpr int CAND_ROW_SHAPES = 5;
+// k_pair_energy shapes (warps per 32 x 32 tile x minimum CTAs per SM) and
+// k_adjoint shapes (minimum CTAs per SM) the autotuner chooses from.
+constexpr int PAIR_SHAPES = 4;
+constexpr int ADJ_SHAPES = 2;
 // Columns (candidates) per work item of the batched triangular solves and
 // the padding unit of the candidate column blocks.
 constexpr int CAND_NC = 16;
@@ -141,6 +145,8 @@ struct Ctx {
     double* red_h = nullptr;    // pinned host mirror of the reduction results
     int* counters = nullptr;    // last-block counters [0,1], abort word [2], wait poll limit [3] of the solves
     int wait_limit = SOLVE_SPIN_LIMIT;
+    int tune_pair = -1, tune_adj = -1;  // autotuned pair-kernel shapes (-1: not yet)
+    float tune_pair_ms[PAIR_SHAPES] = {0}, tune_adj_ms[ADJ_SHAPES] = {0};
     int pivot_mode = 0;         // LDL^H pivots: 0 real (default), 1 complex as the reference keeps them
     cd* yv = nullptr;           // forward-solve result (ld)
     cd* zv = nullptr;           // D^-1 scaled forward result (ld)

@@ -262,9 +262,12 @@ __global__ void __launch_bounds__(128) k_pair_diag(SysParams sp, const double* _
     }
 }
 
-// Off-diagonal pairs k > l, k in [r0, r1): H, S only.
-template <int N>
-__global__ void __launch_bounds__(256) k_pair_energy(SysParams sp, const double* __restrict__ coef,
+// Off-diagonal pairs k > l, k in [r0, r1): H, S only.  One CTA per 32 x 32
+// tile, NW warps (lanes along k, warps along l, 32 / NW columns each); the
+// shape (NW, MINB) is chosen by timing (PAIR_SHAPES); every shape computes
+// each element with the same instructions, so results do not depend on it.
+template <int N, int NW, int MINB>
+__global__ void __launch_bounds__(NW * 32, MINB) k_pair_energy(SysParams sp, const double* __restrict__ coef,
                                                      const cd* __restrict__ bra, const cd* __restrict__ ket,
                                                      const double* __restrict__ detL,
                                                      const double* __restrict__ diagS, cd* __restrict__ H,
@@ -282,8 +285,8 @@ __global__ void __launch_bounds__(256) k_pair_energy(SysParams sp, const double*
     const double dk = detL[k];
     const double dSk = diagS[k];
 #pragma unroll 1
-    for (int j = 0; j < TILE / 8; j++) {
-        const int l = C * TILE + w + 8 * j;
+    for (int j = 0; j < TILE / NW; j++) {
+        const int l = C * TILE + w + NW * j;
         if (l >= k) break;
         const double absdet = fabs(detL[l] * dk);
         cd Hs = mk(0.0, 0.0), Ss = mk(0.0, 0.0);
@@ -409,8 +412,8 @@ struct AdjNV {
     static constexpr int value = 2 * Sym<N>::NP + 1;
 };
 
-template <int N>
-__global__ void __launch_bounds__(256) k_adjoint(SysParams sp, const double* __restrict__ coef,
+template <int N, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_adjoint(SysParams sp, const double* __restrict__ coef,
                                                  const double* __restrict__ Pd, const cd* __restrict__ bra,
                                                  const cd* __restrict__ ket, const double* __restrict__ detL,
                                                  const double* __restrict__ diagS, const cd* __restrict__ cvec,
@@ -1037,15 +1040,78 @@ int launch_pair_diag(Ctx& c, int r0, int r1, double approx_e, int deriv, int nfr
     ECG_DISPATCH_N(c.n, diag_n, c, r0, r1, approx_e, deriv, nfru)
 }
 
+// The pair-kernel shapes the autotuner chooses from: k_pair_energy (warps
+// per tile, minimum CTAs per SM), k_adjoint (minimum CTAs per SM).
+template <int N>
+static void pair_energy_launch(Ctx& c, int v, unsigned grid, int r0, int r1, int Rlo, double approx_e, long long t0)
+{
+    switch (v) {
+        case 0:
+            k_pair_energy<N, 8, 2><<<grid, 256, 0, c.stream>>>(c.sp, c.coef, c.bra, c.ket, c.detL, c.diagS, c.H, c.S,
+                                                               c.ld, r0, r1, Rlo, c.method, approx_e, t0);
+            break;
+        case 1:
+            k_pair_energy<N, 8, 3><<<grid, 256, 0, c.stream>>>(c.sp, c.coef, c.bra, c.ket, c.detL, c.diagS, c.H, c.S,
+                                                               c.ld, r0, r1, Rlo, c.method, approx_e, t0);
+            break;
+        case 2:
+            k_pair_energy<N, 4, 2><<<grid, 128, 0, c.stream>>>(c.sp, c.coef, c.bra, c.ket, c.detL, c.diagS, c.H, c.S,
+                                                               c.ld, r0, r1, Rlo, c.method, approx_e, t0);
+            break;
+        default:
+            k_pair_energy<N, 4, 4><<<grid, 128, 0, c.stream>>>(c.sp, c.coef, c.bra, c.ket, c.detL, c.diagS, c.H, c.S,
+                                                               c.ld, r0, r1, Rlo, c.method, approx_e, t0);
+            break;
+    }
+}
+
+// Time every shape once on this launch (the last run's results stand:
+// all shapes write the same values) and keep the fastest for the context.
+template <typename F>
+static int tune(Ctx& c, int nshapes, int& choice, float* ms_out, F run)
+{
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return -2;
+    float best = 1e30f;
+    int bv = 0;
+    for (int v = 0; v < nshapes; v++) {
+        cudaEventRecord(e0, c.stream);
+        run(v);
+        cudaEventRecord(e1, c.stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return -2;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms_out) ms_out[v] = ms;
+        if (ms < best) {
+            best = ms;
+            bv = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // rerun the chosen shape last unless it already was
+    if (bv != nshapes - 1) run(bv);
+    choice = bv;
+    return last_err();
+}
+
 template <int N>
 static int energy_n(Ctx& c, int r0, int r1, double approx_e)
 {
     if (r1 <= r0) return 0;
     const int Rlo = r0 / TILE, Rhi = (r1 + TILE - 1) / TILE;
     const long long nt = tile_count(Rlo, Rhi);
-    k_pair_energy<N><<<(unsigned)nt, 256, 0, c.stream>>>(c.sp, c.coef, c.bra, c.ket, c.detL, c.diagS, c.H, c.S,
-                                                         c.ld, r0, r1, Rlo, c.method, approx_e, 0LL);
     c.launches++;
+    // shapes are tuned on the first launch with at least 256 tiles
+    if (c.tune_pair < 0 && nt >= 256)
+        return tune(c, PAIR_SHAPES, c.tune_pair, c.tune_pair_ms, [&](int v) {
+            pair_energy_launch<N>(c, v, (unsigned)nt, r0, r1, Rlo, approx_e, 0LL);
+        });
+    pair_energy_launch<N>(c, c.tune_pair < 0 ? 0 : c.tune_pair, (unsigned)nt, r0, r1, Rlo, approx_e, 0LL);
     return last_err();
 }
 int launch_pair_energy(Ctx& c, int r0, int r1, double approx_e) { ECG_DISPATCH_N(c.n, energy_n, c, r0, r1, approx_e) }
@@ -1056,8 +1122,7 @@ static int energy_tiles_n(Ctx& c, int r0, int r1, double approx_e, long long t0,
 {
     if (r1 <= r0 || count <= 0) return 0;
     const int Rlo = r0 / TILE;
-    k_pair_energy<N><<<(unsigned)count, 256, 0, c.stream>>>(c.sp, c.coef, c.bra, c.ket, c.detL, c.diagS, c.H, c.S,
-                                                            c.ld, r0, r1, Rlo, c.method, approx_e, t0);
+    pair_energy_launch<N>(c, c.tune_pair < 0 ? 0 : c.tune_pair, (unsigned)count, r0, r1, Rlo, approx_e, t0);
     c.launches++;
     return last_err();
 }
@@ -1143,12 +1208,25 @@ static int adjoint_n(Ctx& c, int nfru, int nfa, double E)
     const size_t smem = (size_t)8 * TILE * NV * sizeof(double);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_adjoint<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_adjoint<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_adjoint<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_adjoint<N><<<(unsigned)nt, 256, smem, c.stream>>>(c.sp, c.coef, c.Pd, c.bra, c.ket, c.detL, c.diagS, c.c, E,
-                                                        nfru, nfa, Rlo, c.part, 0LL);
+    auto run = [&](int v) {
+        if (v == 0)
+            k_adjoint<N, 1><<<(unsigned)nt, 256, smem, c.stream>>>(c.sp, c.coef, c.Pd, c.bra, c.ket, c.detL, c.diagS,
+                                                                   c.c, E, nfru, nfa, Rlo, c.part, 0LL);
+        else
+            k_adjoint<N, 2><<<(unsigned)nt, 256, smem, c.stream>>>(c.sp, c.coef, c.Pd, c.bra, c.ket, c.detL, c.diagS,
+                                                                   c.c, E, nfru, nfa, Rlo, c.part, 0LL);
+    };
     c.launches++;
+    if (c.tune_adj < 0 && nt >= 256) {
+        const int r = tune(c, ADJ_SHAPES, c.tune_adj, c.tune_adj_ms, run);
+        if (r) return r;
+    } else {
+        run(c.tune_adj < 0 ? 0 : c.tune_adj);
+    }
     const int nf = nfa - nfru;
     k_adjoint_final<N><<<(nf * 32 + 255) / 256, 256, 0, c.stream>>>(c.part, c.params, nfru, nfa, Rlo, Rhi, c.grad);
     c.launches++;
@@ -1166,10 +1244,10 @@ static int adjoint_tiles_n(Ctx& c, int nfru, int nfa, double E, const cd* cvec, 
     if (nfa <= nfru || count <= 0) return 0;
     constexpr int NV = AdjNV<N>::value;
     const size_t smem = (size_t)8 * TILE * NV * sizeof(double);
-    if (cudaFuncSetAttribute(k_adjoint<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (cudaFuncSetAttribute(k_adjoint<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return -2;
-    k_adjoint<N><<<(unsigned)count, 256, smem, c.stream>>>(c.sp, c.coef, c.Pd, c.bra, c.ket, c.detL, c.diagS, cvec,
-                                                           E, nfru, nfa, nfru / TILE, part, t0);
+    k_adjoint<N, 1><<<(unsigned)count, 256, smem, c.stream>>>(c.sp, c.coef, c.Pd, c.bra, c.ket, c.detL, c.diagS,
+                                                              cvec, E, nfru, nfa, nfru / TILE, part, t0);
     c.launches++;
     return last_err();
 }
@@ -1380,12 +1458,12 @@ static int run(const SysParams& sp, const Terms& terms, unsigned char* base, con
     const int Rlo = nfru / TILE, Rhi = (nfa + TILE - 1) / TILE;
     const long long nt = tile_count(Rlo, Rhi);
     const size_t smem = (size_t)8 * TILE * NV * sizeof(double);
-    if (cudaFuncSetAttribute(k_adjoint<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    if (cudaFuncSetAttribute(k_adjoint<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
         return ECG_ECUDA;
     }
-    k_adjoint<N><<<(unsigned)nt, 256, smem, st>>>(sp, coef, Pd, bra, ket, detL, diagS, cvec, E, nfru, nfa, Rlo, part,
-                                                  0LL);
+    k_adjoint<N, 1><<<(unsigned)nt, 256, smem, st>>>(sp, coef, Pd, bra, ket, detL, diagS, cvec, E, nfru, nfa, Rlo, part,
+                                                     0LL);
     const int nf = nfa - nfru;
     k_adjoint_final<N><<<(nf * 32 + 255) / 256, 256, 0, st>>>(part, params, nfru, nfa, Rlo, Rhi, grad);
     return cudaGetLastError() == cudaSuccess ? ECG_OK : ECG_ECUDA;

@@ -58,6 +58,7 @@ PROTOTYPES = {
     "ecg_adjoint_part_doubles": (C.c_int, [_vp, C.POINTER(C.c_longlong)]),
     "ecg_adjoint_tiles": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_longlong, C.c_longlong, C.c_void_p]),
     "ecg_adjoint_finish": (C.c_int, [_vp, C.c_int, C.c_int, C.c_void_p, _dp]),
+    "ecg_get_tuning": (C.c_int, [_vp, _ip, _ip, _ip, _dp]),
     "ecg_set_pivot_mode": (C.c_int, [_vp, C.c_int]),
     "ecg_set_wait_limit": (C.c_int, [_vp, C.c_int]),
     "ecg_io_bytes": (C.c_int, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),

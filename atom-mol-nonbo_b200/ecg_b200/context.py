@@ -391,6 +391,15 @@ class Context:
                "ecg_adjoint_finish")
         return g
 
+    def tuning(self):
+        """The autotuner's choices: dict(pair_shape, adjoint_shape,
+        cand_row_shape, times_ms) (-1: not tuned yet)."""
+        a, b, cc = C.c_int(), C.c_int(), C.c_int()
+        t = np.zeros(6)
+        _check(self.lib.ecg_get_tuning(self.h, C.byref(a), C.byref(b), C.byref(cc), dptr(t)), "ecg_get_tuning")
+        return {"pair_shape": a.value, "adjoint_shape": b.value, "cand_row_shape": cc.value,
+                "pair_shape_ms": t[:4].round(4).tolist(), "adjoint_shape_ms": t[4:].round(4).tolist()}
+
     def set_pivot_mode(self, mode):
         """LDL^H pivots: 0 real (default), 1 complex as the reference."""
         _check(self.lib.ecg_set_pivot_mode(self.h, int(mode)), "ecg_set_pivot_mode")

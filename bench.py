@@ -284,6 +284,7 @@ def run_ours(args, dist):
     dist.barrier()
     launches = ctx.launch_count() - launches0
     clk = clocks.stop()
+    tuning = ctx.tuning()
     ms_step = dist.max(total_ms) / args.steps
     value = dist.sum(args.steps) / (dist.max(total_ms) / 1e3)
 
@@ -398,6 +399,7 @@ def run_ours(args, dist):
         "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": (h1 - h0) // args.steps,
                 "d2h_bytes_per_step": (d1 - d0) // args.steps},
         "gpu_launches": int(launches),
+        "autotune": tuning,
         "roofline": roof_line,
         "clocks": clk,
     }

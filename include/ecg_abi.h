@@ -297,6 +297,18 @@ int ecg_adjoint_tiles(ecg_ctx* ctx, int nfru, int nfa, double energy, long long 
                       void* part_dev);
 int ecg_adjoint_finish(ecg_ctx* ctx, int nfru, int nfa, const void* part_dev, double* grad_host);
 
+/* Shapes the context's autotuner chose (-1: not tuned yet).  The pair
+ * kernels' shape is chosen once per context by timing every candidate
+ * shape on the first large launch (the outputs do not depend on it):
+ *   pair_shape     k_pair_energy, 0..3: warps per 32 x 32 pair tile (8, 8,
+ *                  4, 4) x register budget (2, 3, 2, 4 CTAs per SM);
+ *   adjoint_shape  k_adjoint, 0..1: 1 or 2 CTAs per SM;
+ *   cand_row_shape k_cand_row, 0..4: warps x candidates per warp.
+ * times_ms (may be NULL) receives the 4 + 2 timings of the first two.  No
+ * counterpart in the reference, whose linalg_setparam table
+ * (src/linalg.f90:83-147) is the fixed tuning this replaces. */
+int ecg_get_tuning(ecg_ctx* ctx, int* pair_shape, int* adjoint_shape, int* cand_row_shape, double* times_ms);
+
 /* Pivots of the context's LDL^H factorisations (GHEPIIS, the candidates'
  * bordered step, the 'G' path): mode 0 (default) keeps them real, dropping
  * the rounding-level imaginary part that the complex arithmetic of
