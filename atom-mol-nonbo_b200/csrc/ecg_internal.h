@@ -17,8 +17,11 @@ constexpr int SOLVE_SPIN_LIMIT = 1 << 22;
 
 // LDL^H block size (rows of one panel).
 constexpr int LDL_NB = 64;
-// Rows per column of the buffers of unscaled panel rows (one panel).
-constexpr int LDL_VLD = LDL_NB;
+// Factorisations of at least this many new rows take the panels in pairs
+// with rank-128 trailing updates (ldlh.cu); the buffers of unscaled panel
+// rows hold a pair's rows per column.
+constexpr int LDL_PAIR_MIN = 6000;
+constexpr int LDL_VLD = 2 * LDL_NB;
 
 // Number of 32 x 32 tiles with row-tile index in [Rlo, Rhi) and column-tile
 // index 0..R (lower triangle including diagonal tiles).
@@ -138,7 +141,7 @@ struct Ctx {
     // LDL^H workspace
     cd* dw = nullptr;           // working diagonal (ld)
     cd* linv = nullptr;         // ld x LDL_NB: inverse unit-lower diagonal blocks
-    cd* vbuf = nullptr;         // 3 x LDL_VLD x ld: unscaled panel rows (rotating)
+    cd* vbuf = nullptr;         // 3 x LDL_VLD x ld: unscaled rows of a panel (pair) (rotating)
     int* status = nullptr;      // device status words (see ST_*)
     int* status_h = nullptr;    // pinned host mirror
     double* red = nullptr;      // reduction scratch for the solver (doubles)

@@ -143,3 +143,25 @@ def test_gradient_finite_differences_configuration_2(k4000):
             worst = max(worst, abs(fd - an) / bound)
             assert abs(fd - an) <= bound, (f, m, an, fd, h)
     print(f"64 parameters: worst |fd - analytic| / bound = {worst:.3f}")
+
+
+def test_energy_with_paired_panels_k6100():
+    """Factorisations of 6000 rows or more take the LDL^H panels in pairs
+    (rank-128 trailing updates); the energy at K = 6100 against the
+    oracle's EnergyIAM with the same lambda~."""
+    K = 6100
+    sysm, params = synth.config_basis(2, K=K)
+    e_floor = synth.SYSTEMS["h2_like"]["e_floor"]
+    with Context(sysm, K) as ctx:
+        ctx.set_params(params)
+        ctx.set_vectors(K, last_eigvec=np.ones(K, dtype=np.complex128))
+        E0, _, _ = ctx.energy_ia(1, K, e_floor, -1e-12, max_iter=300, specif_norm=0)
+        lam = E0 * 1.000001
+        ctx.set_vectors(K, last_eigvec=np.ones(K, dtype=np.complex128))
+        E, err, it = ctx.energy_ia(1, K, lam, 1e-12, specif_norm=0)
+    o = orc.Oracle(sysm, K)
+    o.set_params(params)
+    o.last[:K] = 1.0
+    Eo, erro, ito = o.energy_ia(1, K, lam, 1e-12, specif_norm=0)
+    print(f"K {K}: E_gpu {E:.15f} E_oracle {Eo:.15f} dE {E - Eo:.2e} codes {err}/{erro} iters {it}/{ito}")
+    assert abs(E - Eo) <= TOL_E
