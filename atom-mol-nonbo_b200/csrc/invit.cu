@@ -187,7 +187,6 @@ __device__ __forceinline__ bool wait_panel(const unsigned* flags, int a, unsigne
                     g = 0;
                     break;
                 }
-                __nanosleep(64);
             }
             if (!g) {
                 atomicExch(status + ST_SOLVE_TIMEOUT, 1);
@@ -231,6 +230,9 @@ __global__ void __launch_bounds__(256) k_fwd_coop(const cd* __restrict__ A, int 
     const int j0 = bstart[j], j1 = bstart[j + 1], b = j1 - j0;
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     load_linv(linv, j0, b, Ls);
+    // this panel's right-hand side and pivots, read before the waits
+    const cd wj = (threadIdx.x < b) ? ld2(w + j0 + threadIdx.x) : mk(0.0, 0.0);
+    const cd dj = (threadIdx.x < b) ? ld2(invD + j0 + threadIdx.x) : mk(0.0, 0.0);
     // lane-partials for the 8 columns this warp owns
     cd acc[8];
 #pragma unroll
@@ -269,7 +271,7 @@ __global__ void __launch_bounds__(256) k_fwd_coop(const cd* __restrict__ A, int 
     __syncthreads();
     if (threadIdx.x < b) {
         const cd s = mk(red[threadIdx.x].x, red[threadIdx.x].y);
-        const cd v = ld2(w + j0 + threadIdx.x) - s;
+        const cd v = wj - s;
         t[threadIdx.x] = make_double2(v.x, v.y);
     }
     __syncthreads();
@@ -291,9 +293,10 @@ __global__ void __launch_bounds__(256) k_fwd_coop(const cd* __restrict__ A, int 
 #pragma unroll
         for (int g = 0; g < 4; g++) s = s + mk(red[g * LDL_NB + r].x, red[g * LDL_NB + r].y);
         y[j0 + r] = s;
-        z[j0 + r] = cmul(s, ld2(invD + j0 + r));
-        __threadfence();
+        z[j0 + r] = cmul(s, dj);
     }
+    // the release by thread 0 after the barrier publishes every thread's
+    // stores above (cumulativity of the gpu-scope release)
     __syncthreads();
     if (threadIdx.x == 0) st_release(flags + j, epoch);
 }
@@ -312,6 +315,7 @@ __global__ void __launch_bounds__(256) k_bwd_coop(const cd* __restrict__ A, int 
     const int j0 = bstart[j], j1 = bstart[j + 1], b = j1 - j0;
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     load_linv(linv, j0, b, Ls);
+    const cd zj = (threadIdx.x < b) ? ld2(z + j0 + threadIdx.x) : mk(0.0, 0.0);  // read before the waits
     cd a0 = mk(0.0, 0.0), a1 = mk(0.0, 0.0);  // rows lane, lane + 32
     bool ok = true;
     for (int c = nb - 1; c > j; c--) {
@@ -342,7 +346,7 @@ __global__ void __launch_bounds__(256) k_bwd_coop(const cd* __restrict__ A, int 
         cd s = mk(0.0, 0.0);
 #pragma unroll
         for (int q = 0; q < 8; q++) s = s + mk(red[q * LDL_NB + r].x, red[q * LDL_NB + r].y);
-        const cd v = ld2(z + j0 + r) - s;
+        const cd v = zj - s;
         t[r] = make_double2(v.x, v.y);
     }
     __syncthreads();
@@ -363,7 +367,6 @@ __global__ void __launch_bounds__(256) k_bwd_coop(const cd* __restrict__ A, int 
 #pragma unroll
         for (int g = 0; g < 4; g++) s = s + mk(red[g * LDL_NB + r].x, red[g * LDL_NB + r].y);
         x[j0 + r] = s;
-        __threadfence();
     }
     __syncthreads();
     if (threadIdx.x == 0) st_release(flags + j, epoch);
