@@ -1008,6 +1008,11 @@ int eval_candidates(Ctx& c, int nbase, int count, const double* cand_host, doubl
                                      c.stream))))
             return r;
         if ((r = CKc(cudaStreamSynchronize(c.stream)))) return r;
+        if (c.status_h[ST_SOLVE_TIMEOUT]) {
+            c.fact_n = 0;
+            c.blk_start.clear();
+            return ECG_ECUDA;
+        }
         if (c.status_h[ST_ZERO_PIVOT] != 0) {
             c.fact_n = 0;
             c.blk_start.clear();

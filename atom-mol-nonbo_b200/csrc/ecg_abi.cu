@@ -68,9 +68,13 @@ void free_ctx(Ctx& c)
                     c.zv, c.spart, c.colval, c.dblk, c.flags};
     for (void* p : ptrs)
         if (p) cudaFree(p);
-    for (auto& g : c.ldl_graphs)
+    for (auto& g : c.ldl_graphs) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.tasks) cudaFree(g.tasks);
+    }
     c.ldl_graphs.clear();
+    if (c.lp_cnt) cudaFree(c.lp_cnt);
+    if (c.lp_direct) cudaFree(c.lp_direct);
     cand_free(c.cand);
     if (c.bounds_h) cudaFreeHost(c.bounds_h);
     if (c.status_h) cudaFreeHost(c.status_h);
@@ -147,6 +151,12 @@ int ghepiis_core(Ctx& c, int k, int n, double apprlambda, double tol, int max_it
     c.bytes_d2h += ST_COUNT * sizeof(int);
     CK(cudaStreamSynchronize(c.stream));
     mark(c, 2);
+    if (c.status_h[ST_SOLVE_TIMEOUT]) {
+        // a bounded wait of the factorisation ran out: no factor
+        c.fact_n = 0;
+        c.blk_start.clear();
+        return ECG_ECUDA;
+    }
     if (c.status_h[ST_ZERO_PIVOT] != 0) {
         // LDLHF returned ErrorCode = 1 (src/linalg.f90:377-380); the factor
         // is incomplete, so no row of it may be reused.
@@ -220,6 +230,7 @@ int g_count(Ctx& c, int n, double sigma, int* nu, int* zero)
     CK(cudaMemcpyAsync(c.status_h, c.status, ST_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
     c.g_last_factorizations++;
+    if (c.status_h[ST_SOLVE_TIMEOUT]) return ECG_ECUDA;
     *nu = c.gcnt_h[0];
     *zero = c.status_h[ST_ZERO_PIVOT] != 0;
     return 0;
@@ -248,8 +259,10 @@ int energy_ga(Ctx& c, int nmin, int nmax, int needed, int which, int want_vector
     CKR(ldlh_factor(c, 0, n));
     CKR(g_inertia(c, n));
     CK(cudaMemcpyAsync(c.gcnt_h, c.gcnt, 2 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(c.status_h, c.status, ST_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
     c.g_last_factorizations++;
+    if (c.status_h[ST_SOLVE_TIMEOUT]) return ECG_ECUDA;
     if (c.gcnt_h[1] < n) return n + c.gcnt_h[1] + 1;
     // initial bracket around the previous eigenvalue, or below min diag(H)
     // (the lowest eigenvalue is at most every diagonal Rayleigh quotient)
@@ -675,6 +688,23 @@ int ecg_set_pivot_mode(ecg_ctx* ctx, int mode)
         c.blk_start.clear();
     }
     return ECG_OK;
+}
+
+int ecg_set_factor_mode(ecg_ctx* ctx, int mode)
+{
+    if (!ctx || mode < 0 || mode > 1) return ECG_EARG;
+    ctx->c.factor_mode = mode;
+    return ECG_OK;
+}
+
+int ecg_factor_trace(ecg_ctx* ctx, int n, unsigned long long* records, long long cap, long long* count)
+{
+    if (!ctx || !count || n < 1 || n > ctx->c.ld) return ECG_EARG;
+    Ctx& c = ctx->c;
+    CK(cudaMemsetAsync(c.status, 0, ST_COUNT * sizeof(int), c.stream));
+    const int r = ldlh_factor_traced(c, n, records, cap, count);
+    if (r == -3) return ECG_ENOMEM;
+    return r ? ECG_ECUDA : ECG_OK;
 }
 
 int ecg_set_wait_limit(ecg_ctx* ctx, int polls)

@@ -165,11 +165,19 @@ struct Ctx {
         std::vector<int> key;
         cudaGraphExec_t exec = nullptr;
         long long launches = 0;  // kernel launches one replay performs
+        unsigned* tasks = nullptr;  // task list of a persistent factorisation (ldlp.cu), owned
     };
     long long graph_launches = 0;
     std::vector<LdlGraph> ldl_graphs;
     int* bounds_h = nullptr;    // pinned staging of the panel boundaries (ld + 2)
     int fact_n = 0;             // rows covered by the current factor
+    // persistent factorisation of whole matrices (ldlp.cu)
+    int factor_mode = 0;        // 0: persistent kernel for m0 = 0, 1: one launch per panel step
+    int lp_grid = 0;            // co-resident CTAs of the persistent kernel (0: not yet known)
+    unsigned* lp_cnt = nullptr; // tile counters, then the next-task counter and the abort word
+    size_t lp_cap = 0;          // capacity of lp_cnt (unsigned)
+    unsigned* lp_direct = nullptr;  // task list of the uncaptured fallback, for lp_direct_n rows
+    int lp_direct_n = 0, lp_direct_count = 0;
 
     // bookkeeping
     long long launches = 0;
@@ -255,6 +263,16 @@ int g_inertia(Ctx& c, int n);
 
 // ---- launchers (ldlh.cu) ----
 int ldlh_factor(Ctx& c, int m0, int n);
+
+// ---- persistent factorisation (ldlp.cu) ----
+int ldlp_grid(Ctx& c);
+int ldlp_tasks(Ctx& c, int n, unsigned** tasks, int* count);
+long long ldlp_task_total(int n);
+int ldlp_reserve(Ctx& c, int np);
+void ldlp_enqueue(Ctx& c, int n, const unsigned* tasks, int ntasks, unsigned long long* trace = nullptr);
+// One persistent factorisation of rows 0..n-1 of the current matrix with a
+// per-task timing record (4 values per task, see ecg_factor_trace).
+int ldlh_factor_traced(Ctx& c, int n, unsigned long long* out, long long cap, long long* count);
 
 // ---- launchers (invit.cu) ----
 int invit_step(Ctx& c, int n, bool first);

@@ -624,24 +624,44 @@ static void enqueue_factor(Ctx& c, int m0, int n, const std::vector<int>& starts
     }
 }
 
+// A whole factorisation (m0 = 0) as one persistent kernel (ldlp.cu): the
+// working upper triangle and diagonal, the tile tasks, then the inverse
+// diagonal blocks of the solves.
+static void enqueue_persist(Ctx& c, int n, const unsigned* tasks, int ntasks, unsigned long long* trace = nullptr)
+{
+    const int ct1 = (n + 31) / 32;
+    k_ldl_mirror<<<dim3(ct1, ct1), 256, 0, c.stream>>>(c.F, c.ld, 0, n, c.dw, 0);
+    c.launches++;
+    ldlp_enqueue(c, n, tasks, ntasks, trace);
+    const int nblk = (n + LDL_NB - 1) / LDL_NB;
+    k_ldl_linv<<<nblk, 256, 2 * LDL_NB * DG_LD * sizeof(double2), c.stream>>>(c.F, c.ld, c.dblk, 0, c.linv);
+    c.launches++;
+}
+
+static void ldl_attrs()
+{
+    if (g_ldl_attr) return;
+    const size_t sm1 = LDL_NB * DG_LD * sizeof(double2);
+    cudaFuncSetAttribute(k_ldl_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+    cudaFuncSetAttribute(k_ldl_diag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DG_SMEM);
+    cudaFuncSetAttribute(k_ldl_diag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DG_SMEM);
+    cudaFuncSetAttribute(k_ldl_linv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * sm1));
+    cudaFuncSetAttribute(k_ldl_bulk<32, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem<32>());
+    cudaFuncSetAttribute(k_ldl_bulk<16, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem<16>());
+    g_ldl_attr = true;
+}
+
 // Factorise rows m0..n-1 of M = H - lambda~ S given the factor of rows
 // 0..m0-1.  The launch sequence depends only on (m0, n) and the existing
 // panel boundaries, so it is captured once into a CUDA graph (both streams)
-// and replayed.
+// and replayed.  A whole factorisation (m0 = 0) runs as the persistent
+// kernel of ldlp.cu unless ecg_set_factor_mode selected the launch-per-panel
+// form.
 int ldlh_factor(Ctx& c, int m0, int n)
 {
     if (m0 < 0 || m0 > n || n > c.ld) return -1;
     if (m0 > c.fact_n) return -1;
-    const size_t sm1 = LDL_NB * DG_LD * sizeof(double2);
-    if (!g_ldl_attr) {
-        cudaFuncSetAttribute(k_ldl_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
-        cudaFuncSetAttribute(k_ldl_diag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DG_SMEM);
-        cudaFuncSetAttribute(k_ldl_diag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DG_SMEM);
-        cudaFuncSetAttribute(k_ldl_linv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * sm1));
-        cudaFuncSetAttribute(k_ldl_bulk<32, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem<32>());
-        cudaFuncSetAttribute(k_ldl_bulk<16, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem<16>());
-        g_ldl_attr = true;
-    }
+    ldl_attrs();
     // block list: existing blocks truncated at m0, then new 64-row blocks
     std::vector<int> starts;
     for (int s : c.blk_start)
@@ -655,18 +675,36 @@ int ldlh_factor(Ctx& c, int m0, int n)
     if (cudaMemcpyAsync(c.dblk, c.bounds_h, (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, c.stream) !=
         cudaSuccess)
         return -2;
-    std::vector<int> key = {m0, n, c.pivot_mode};
+    // whole factorisations take the persistent kernel below LDL_PAIR_MIN
+    // rows (at 10000 rows the panel pairs' rank-128 launches measured 57.2
+    // against its 59.4 ms)
+    const bool persist = (m0 == 0 && n > 0 && n < LDL_PAIR_MIN && c.factor_mode == 0 && ldlp_grid(c) > 0);
+    std::vector<int> key = {m0, n, c.pivot_mode, persist ? 1 : 0};
     key.insert(key.end(), starts.begin(), starts.begin() + nexist);
     Ctx::LdlGraph* g = nullptr;
     for (auto& e : c.ldl_graphs)
         if (e.key == key) g = &e;
     if (!g) {
+        unsigned* tasks = nullptr;
+        int ntasks = 0;
+        if (persist) {
+            const int r = ldlp_reserve(c, nb);
+            if (r) return r;
+            const int t = ldlp_tasks(c, n, &tasks, &ntasks);
+            if (t) return t;
+        }
+        auto enqueue = [&]() {
+            if (persist)
+                enqueue_persist(c, n, tasks, ntasks);
+            else
+                enqueue_factor(c, m0, n, starts, nexist);
+        };
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         bool ok = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
         if (ok) {
             const long long l0 = c.launches;
-            enqueue_factor(c, m0, n, starts, nexist);
+            enqueue();
             c.graph_launches = c.launches - l0;
             c.launches = l0;
             ok = cudaStreamEndCapture(c.stream, &graph) == cudaSuccess && graph &&
@@ -676,26 +714,90 @@ int ldlh_factor(Ctx& c, int m0, int n)
         if (!ok) {
             cudaGetLastError();
             if (exec) cudaGraphExecDestroy(exec);
-            // capture unavailable: run the launches directly
-            enqueue_factor(c, m0, n, starts, nexist);
+            // capture unavailable: run the launches directly (a persistent
+            // factorisation keeps its task list until the next one)
+            if (persist) {
+                if (c.lp_direct) {
+                    cudaStreamSynchronize(c.stream);
+                    cudaFree(c.lp_direct);
+                }
+                c.lp_direct = tasks;
+                c.lp_direct_n = n;
+                c.lp_direct_count = ntasks;
+            }
+            enqueue();
             if (cudaGetLastError() != cudaSuccess) return -2;
             c.blk_start = starts;
             c.fact_n = n;
             return 0;
         }
         if (c.ldl_graphs.size() >= 8) {
+            cudaStreamSynchronize(c.stream);
             cudaGraphExecDestroy(c.ldl_graphs.front().exec);
+            if (c.ldl_graphs.front().tasks) cudaFree(c.ldl_graphs.front().tasks);
             c.ldl_graphs.erase(c.ldl_graphs.begin());
         }
         c.ldl_graphs.push_back({key, exec});
         g = &c.ldl_graphs.back();
         g->launches = c.graph_launches;
+        g->tasks = tasks;
     }
     if (cudaGraphLaunch(g->exec, c.stream) != cudaSuccess) return -2;
     c.launches += g->launches;
     c.blk_start = starts;
     c.fact_n = n;
     return 0;
+}
+
+// One persistent factorisation of rows 0..n-1 of the matrix in F's lower
+// triangle, outside any graph, with a timing record per task: out receives
+// 4 values per task (code | CTA << 32 | panels applied << 48, then the
+// globaltimer in ns when the CTA began waiting for the task's tiles, when
+// they were ready, when the task was published).  The factor is left as
+// ldlh_factor(c, 0, n) leaves it.
+int ldlh_factor_traced(Ctx& c, int n, unsigned long long* out, long long cap, long long* count)
+{
+    if (n < 1 || n > c.ld) return -1;
+    if (ldlp_grid(c) <= 0) return -1;
+    const int nb = (n + LDL_NB - 1) / LDL_NB;
+    ldl_attrs();
+    std::vector<int> starts;
+    for (int s = 0; s < n; s += LDL_NB) starts.push_back(s);
+    for (int i = 0; i < nb; i++) c.bounds_h[i] = starts[i];
+    c.bounds_h[nb] = n;
+    if (cudaMemcpyAsync(c.dblk, c.bounds_h, (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, c.stream) !=
+        cudaSuccess)
+        return -2;
+    if (ldlp_reserve(c, nb)) return -3;
+    unsigned* tasks = nullptr;
+    int ntasks = 0;
+    if (ldlp_tasks(c, n, &tasks, &ntasks)) return -2;
+    const long long total = ldlp_task_total(n);
+    unsigned long long* d = nullptr;
+    if (cudaMalloc(&d, (size_t)total * 4 * sizeof(unsigned long long)) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(tasks);
+        return -3;
+    }
+    enqueue_persist(c, n, tasks, ntasks, d);
+    unsigned recs = 0;
+    const size_t ntile = (size_t)nb * (nb + 1) / 2;
+    int r = 0;
+    if (cudaMemcpyAsync(&recs, c.lp_cnt + ntile + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, c.stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(c.stream) != cudaSuccess)
+        r = -2;
+    if (!r) {
+        *count = recs;
+        if (out && cap >= (long long)recs * 4 &&
+            cudaMemcpy(out, d, (size_t)recs * 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+            r = -2;
+    }
+    cudaFree(d);
+    cudaFree(tasks);
+    c.blk_start = starts;
+    c.fact_n = n;
+    return r;
 }
 
 }  // namespace ecg

@@ -1,0 +1,1008 @@
+// ldlp.cu -- LDL^H factorisation of a whole matrix (no existing rows) as one
+// persistent cooperative kernel over 64 x 64 tiles, the drop-in for LDLHF
+// with m = 1 (src/linalg.f90:316-455).
+//
+// Same storage contract and recurrence as ldlh.cu: M's lower triangle is left
+// untouched, the strict upper triangle receives L^H, invD receives 1/d; the
+// working Schur complement W(r, c), r < c, lives in the upper triangle and
+// its diagonal in dw.  The factorisation is split into tasks on 64 x 64 tiles
+// (R, C), R <= C, of panel index s:
+//   D(s)        eliminate the diagonal tile (s, s): U_ss, invD, pivots d_s
+//               (written to dw over the consumed working diagonal);
+//   T(s, C)     panel rows of tile (s, C) by substitution with U_ss:
+//               U(s, C) = invD L_ss^-1 W(s, C);
+//   B(s, R, C)  W(R, C) -= conj(U(s, R))^T diag(d_s) U(s, C), s < R <= C
+//               (the unscaled rows of the reference's recurrence, d U, are
+//               formed in registers from U and d instead of being stored).
+// Every tile has a counter: the number of panels applied to it (D and T set
+// it to s + 1 when the tile is final).  A task waits (bounded) until its
+// tiles carry the counts it needs:
+//   D(s): cnt(s,s) >= s;  T(s,C): cnt(s,s) >= s+1, cnt(s,C) >= s;
+//   B(s,R,C): cnt(s,R) >= s+1, cnt(s,C) >= s+1, cnt(R,C) >= s.
+// The CTAs (all co-resident: cooperative launch) take tasks from a list in
+// a fixed order through one atomic counter.  The list is a topological order
+// of that dependency graph, made on the host by list scheduling on as many
+// simulated workers as the grid has CTAs, always starting the ready task
+// with the longest remaining path (upward rank), so the chain D(s) -> T(s,
+// s+1) -> B(s, s+1, s+1) -> D(s+1) goes first and the trailing updates fill
+// the rest.  Because every task's dependencies come earlier in the list and
+// every CTA is resident, the earliest unfinished task can always proceed:
+// the kernel cannot deadlock.  Waits are still bounded (the poll limit of
+// ecg_set_wait_limit); a CTA that gives up records ST_SOLVE_TIMEOUT and
+// sets the abort word, after which every CTA stops taking tasks.
+#include <algorithm>
+#include <queue>
+#include <utility>
+#include <vector>
+#include "ecg_internal.h"
+#include "zmma.cuh"
+
+namespace ecg {
+
+constexpr unsigned LP_D = 0, LP_T = 1, LP_B = 2;
+constexpr unsigned LP_NONE = 0xffffffffu;
+constexpr int LP_KC = 16;          // k rows per cp.async stage of an update
+constexpr int LP_P = 66;           // pitch (double2) of the staged operands: 2 mod 8, conflict-free fragments
+constexpr int LP_ST = 3;           // stages
+constexpr int LP_LD = LDL_NB + 1;  // pitch of the 64 x 64 shared tiles of D and T
+constexpr int LP_SUB = 8;          // sub-panel rows of the diagonal elimination
+constexpr int LP_MERGE = 4;        // most panels one trailing update applies at once
+constexpr size_t LP_SMEM_B = (size_t)(LP_ST * LP_KC * 2 * LP_P + LP_MERGE * LDL_NB) * sizeof(double2);
+constexpr size_t LP_SMEM_D = (size_t)(LDL_NB * LP_LD + LP_SUB * LDL_NB) * sizeof(double2);
+
+__host__ __device__ __forceinline__ unsigned lp_code(unsigned type, int s, int R, int C)
+{
+    return type << 30 | (unsigned)s << 20 | (unsigned)R << 10 | (unsigned)C;
+}
+// counter of tile (R, C), R <= C: column-wise packed triangle
+__host__ __device__ __forceinline__ long long lp_tix(int R, int C) { return (long long)C * (C + 1) / 2 + R; }
+
+// ---------------------------------------------------------------------------
+// Host: the task list.
+// ---------------------------------------------------------------------------
+// Task durations (us) for the list scheduler, as measured on a B200 with
+// two CTAs per SM (globaltimer records of ecg_factor_trace); only their
+// ratios and the resulting priorities matter.
+struct LpCost {
+    double d = 28.0, t = 18.0, b = 24.0, bd = 18.0;
+};
+
+// Tasks of a factorisation with np panels for a grid of P CTAs: the list
+// the CTAs other than the chain CTA take, and (if full is given) every task
+// in the simulated start order, the chain's included.
+static std::vector<unsigned> lp_schedule(int np, int P, const LpCost& cost, std::vector<unsigned>* full = nullptr)
+{
+    std::vector<unsigned> code;
+    std::vector<long long> idD(np), baseB(np);
+    std::vector<long long> idT((size_t)np * np, -1);
+    for (int s = 0; s < np; s++) {
+        idD[s] = (long long)code.size();
+        code.push_back(lp_code(LP_D, s, s, s));
+        for (int C = s + 1; C < np; C++) {
+            idT[(size_t)s * np + C] = (long long)code.size();
+            code.push_back(lp_code(LP_T, s, s, C));
+        }
+        baseB[s] = (long long)code.size();
+        for (int R = s + 1; R < np; R++)
+            for (int C = R; C < np; C++) code.push_back(lp_code(LP_B, s, R, C));
+    }
+    auto idB = [&](int s, int R, int C) -> long long {
+        const long long off = (long long)(R - s - 1) * np - ((long long)(R - 1) * R / 2 - (long long)s * (s + 1) / 2);
+        return baseB[s] + off + (C - R);
+    };
+    const long long N = (long long)code.size();
+    // predecessors (at most three) in creation order, which is topological
+    std::vector<long long> pred((size_t)N * 3, -1);
+    std::vector<double> w((size_t)N);
+    for (long long t = 0; t < N; t++) {
+        const unsigned c = code[t];
+        const int type = c >> 30, s = (c >> 20) & 1023, R = (c >> 10) & 1023, C = c & 1023;
+        long long* p = &pred[(size_t)t * 3];
+        if (type == LP_D) {
+            if (s > 0) p[0] = idB(s - 1, s, s);
+            w[t] = cost.d;
+        } else if (type == LP_T) {
+            p[0] = idD[s];
+            if (s > 0) p[1] = idB(s - 1, s, C);
+            w[t] = cost.t;
+        } else {
+            p[0] = idT[(size_t)s * np + R];
+            if (C != R) p[1] = idT[(size_t)s * np + C];
+            if (s > 0) p[2] = idB(s - 1, R, C);
+            w[t] = (R == C) ? cost.bd : cost.b;
+        }
+    }
+    // successors (CSR)
+    std::vector<long long> so((size_t)N + 1, 0), sl;
+    for (long long t = 0; t < N; t++)
+        for (int k = 0; k < 3; k++)
+            if (pred[(size_t)t * 3 + k] >= 0) so[(size_t)pred[(size_t)t * 3 + k] + 1]++;
+    for (long long t = 0; t < N; t++) so[(size_t)t + 1] += so[(size_t)t];
+    sl.resize((size_t)so[(size_t)N]);
+    {
+        std::vector<long long> fill(so.begin(), so.end() - 1);
+        for (long long t = 0; t < N; t++)
+            for (int k = 0; k < 3; k++) {
+                const long long p = pred[(size_t)t * 3 + k];
+                if (p >= 0) sl[(size_t)fill[(size_t)p]++] = t;
+            }
+    }
+    // upward rank: own duration plus the longest path through the successors
+    std::vector<double> rank((size_t)N);
+    for (long long t = N - 1; t >= 0; t--) {
+        double m = 0.0;
+        for (long long e = so[(size_t)t]; e < so[(size_t)t + 1]; e++) m = std::max(m, rank[(size_t)sl[(size_t)e]]);
+        rank[(size_t)t] = w[(size_t)t] + m;
+    }
+    // list scheduling: the chain worker runs D(s), T(s, s+1), B(s, s+1,
+    // s+1) in that order, each as soon as it is ready; P - 1 list workers
+    // start the ready task of highest rank (earliest created among equals)
+    // whenever one of them is free.  `full` receives every task in start
+    // order, the returned list the tasks of the list workers.
+    std::vector<char> chain((size_t)N, 0);
+    std::vector<long long> cseq;
+    for (int s = 0; s < np; s++) {
+        chain[(size_t)idD[s]] = 1;
+        cseq.push_back(idD[s]);
+        if (s + 1 < np) {
+            const long long t = idT[(size_t)s * np + s + 1], b = idB(s, s + 1, s + 1);
+            chain[(size_t)t] = chain[(size_t)b] = 1;
+            cseq.push_back(t);
+            cseq.push_back(b);
+        }
+    }
+    std::vector<int> npred((size_t)N, 0);
+    for (long long t = 0; t < N; t++)
+        for (int k = 0; k < 3; k++) npred[(size_t)t] += pred[(size_t)t * 3 + k] >= 0;
+    typedef std::pair<double, long long> Item;
+    std::priority_queue<Item> ready;                                        // (rank, -id)
+    std::priority_queue<Item, std::vector<Item>, std::greater<Item>> busy;  // (finish, id)
+    for (long long t = 0; t < N; t++)
+        if (npred[(size_t)t] == 0 && !chain[(size_t)t]) ready.push({rank[(size_t)t], -t});
+    std::vector<unsigned> order;
+    order.reserve((size_t)N);
+    if (full) {
+        full->clear();
+        full->reserve((size_t)N);
+    }
+    int free_w = std::max(1, P - 1);
+    bool chain_free = true;
+    size_t ci = 0;
+    long long started = 0;
+    double now = 0.0;
+    while (started < N) {
+        if (chain_free && ci < cseq.size() && npred[(size_t)cseq[ci]] == 0) {
+            const long long t = cseq[ci];
+            if (full) full->push_back(code[(size_t)t]);
+            busy.push({now + w[(size_t)t], t});
+            chain_free = false;
+            started++;
+        }
+        while (free_w > 0 && !ready.empty()) {
+            const long long t = -ready.top().second;
+            ready.pop();
+            order.push_back(code[(size_t)t]);
+            if (full) full->push_back(code[(size_t)t]);
+            busy.push({now + w[(size_t)t], t});
+            free_w--;
+            started++;
+        }
+        if (busy.empty()) break;  // cannot happen for a valid graph
+        const Item f = busy.top();
+        busy.pop();
+        now = f.first;
+        if (chain[(size_t)f.second]) {
+            chain_free = true;
+            ci++;
+        } else {
+            free_w++;
+        }
+        for (long long e = so[(size_t)f.second]; e < so[(size_t)f.second + 1]; e++) {
+            const long long q = sl[(size_t)e];
+            if (--npred[(size_t)q] == 0 && !chain[(size_t)q]) ready.push({rank[(size_t)q], -q});
+        }
+    }
+    return order;
+}
+
+// ---------------------------------------------------------------------------
+// Device.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned lp_ld_acquire(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void lp_st_release(unsigned* p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ double2 lp_ldcg(const cd* p) { return __ldcg(reinterpret_cast<const double2*>(p)); }
+__device__ __forceinline__ void lp_mma(double& c0, double& c1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+__device__ __forceinline__ cd lp_shfl(cd v, int src)
+{
+    return cd{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
+}
+
+// Thread 0: wait until *p >= v.  False when this CTA must stop (the poll
+// limit ran out here or the abort word is set).
+__device__ __forceinline__ bool lp_wait(const unsigned* p, unsigned v, unsigned* ctl, int* status, int limit)
+{
+    int spins = 0;
+    while (lp_ld_acquire(p) < v) {
+        if (++spins > limit || *((volatile unsigned*)(ctl + 1)) != 0u) {
+            atomicExch(status + ST_SOLVE_TIMEOUT, 1);
+            atomicExch(ctl + 1, 1u);
+            return false;
+        }
+        __nanosleep(32);
+    }
+    return true;
+}
+
+// D(s): the diagonal tile by 8-row sub-panels in shared memory, as
+// k_ldl_diag does (ldlh.cu), with the 8 x 8 elimination spread over the
+// lanes of warp 0 (lane j owns column j of the sub-block; the pivot and the
+// rows of U reach the other lanes by shuffles).  Per pivot q the operations
+// and their order are those of the single-thread form: u_j = W(q, j) / d,
+// W(i, j) -= conj(u_i) W(q, j).
+template <bool CPLX>
+__device__ void lp_diag(cd* __restrict__ A, int ld, int n, int s, cd* __restrict__ dw, cd* __restrict__ invD,
+                        int* __restrict__ status, double2* sm)
+{
+    double2* Ws = sm;                   // Ws[r * LP_LD + c], r <= c
+    double2* Wu = sm + LDL_NB * LP_LD;  // Wu[q * 64 + c]: unscaled rows of the sub-panel
+    __shared__ double2 sid[LP_SUB];
+    const int p0 = s * LDL_NB, b = min(LDL_NB, n - p0);
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
+        const int r = e & 63, c = e >> 6;
+        double2 v = make_double2(0.0, 0.0);
+        if (r < b && c < b) {
+            if (r < c)
+                v = lp_ldcg(A + (size_t)(p0 + r) + (size_t)(p0 + c) * ld);
+            else if (r == c)
+                v = lp_ldcg(dw + p0 + r);
+        }
+        Ws[r * LP_LD + c] = v;
+    }
+    __syncthreads();
+    // 8 x 8 elimination of the sub-block at s0 by the 32 lanes of warp 0
+    auto eliminate = [&](int s0) {
+        const int nq = min(LP_SUB, b - s0);
+        const int j = lane;
+        const bool col = j < nq;
+        cd a[LP_SUB];
+#pragma unroll
+        for (int i = 0; i < LP_SUB; i++) {
+            double2 v = make_double2(0.0, 0.0);
+            if (col && i <= j) v = Ws[(s0 + i) * LP_LD + s0 + j];
+            a[i] = cd{v.x, v.y};
+        }
+#pragma unroll
+        for (int q = 0; q < LP_SUB; q++) {
+            if (q < nq) {
+                const cd dq = lp_shfl(a[q], q);  // W(q, q) from lane q
+                const double dr = dq.x, di = CPLX ? dq.y : 0.0;
+                const bool zero = (dr == 0.0 && di == 0.0);
+                double id, idi = 0.0;
+                if (CPLX) {
+                    const double m = zero ? 0.0 : __drcp_rn(fma(dr, dr, di * di));
+                    id = dr * m;
+                    idi = -di * m;
+                } else {
+                    id = zero ? 0.0 : __drcp_rn(dr);
+                }
+                if (lane == 0) {
+                    sid[q] = make_double2(id, idi);
+                    invD[p0 + s0 + q] = cd{id, idi};
+                    dw[p0 + s0 + q] = cd{dr, di};  // the pivot, for the trailing updates
+                    if (zero) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + s0 + q + 1);
+                }
+                cd u = cd{0.0, 0.0};
+                if (col && j > q) u = CPLX ? cmul(a[q], cd{id, idi}) : cd{a[q].x * id, a[q].y * id};  // U(q, j)
+#pragma unroll
+                for (int i = q + 1; i < LP_SUB; i++) {
+                    const cd ui = lp_shfl(u, i);
+                    if (col && j >= i) a[i] = cfms(conj(ui), a[q], a[i]);
+                }
+                if (col && j > q) a[q] = u;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < LP_SUB; i++)
+            if (col && i < j) Ws[(s0 + i) * LP_LD + s0 + j] = make_double2(a[i].x, a[i].y);
+    };
+    if (wp == 0) eliminate(0);
+    __syncthreads();
+    for (int s0 = 0; s0 < b; s0 += LP_SUB) {
+        const int nq = min(LP_SUB, b - s0);
+        // (b) sub-panel rows beyond the sub-block, one thread per column
+        const int t0 = s0 + LP_SUB;
+        if (t0 < b && tid < b - t0) {
+            const int c = t0 + tid;
+            cd wun[LP_SUB];
+#pragma unroll
+            for (int q = 0; q < LP_SUB; q++) {
+                if (q < nq) {
+                    const double2 w = Ws[(s0 + q) * LP_LD + c];
+                    cd v = cd{w.x, w.y};
+#pragma unroll
+                    for (int q2 = 0; q2 < q; q2++) {
+                        const double2 u = Ws[(s0 + q2) * LP_LD + s0 + q];  // U(q2, q)
+                        v = cfms(cd{u.x, -u.y}, wun[q2], v);
+                    }
+                    wun[q] = v;
+                    Wu[q * LDL_NB + c] = make_double2(v.x, v.y);
+                    const double2 id = sid[q];
+                    const cd uq = CPLX ? cmul(v, cd{id.x, id.y}) : cd{v.x * id.x, v.y * id.x};
+                    Ws[(s0 + q) * LP_LD + c] = make_double2(uq.x, uq.y);
+                } else {
+                    wun[q] = cd{0.0, 0.0};
+                }
+            }
+        }
+        __syncthreads();
+        // (c) rank-8 update beyond the sub-panel on the FP64 tensor cores;
+        // warp 0 takes the next diagonal sub-block and eliminates it at once
+        if (t0 < b) {
+            const int g = lane >> 2, t4 = lane & 3;
+            const int T = (b - t0 + 7) >> 3;
+            const int ntiles = T * (T + 1) / 2;
+            for (int tile = (wp == 0) ? 0 : wp; tile < ntiles; tile += (wp == 0) ? ntiles : 7) {
+                int Rr = 0, rem = tile;
+                while (rem >= T - Rr) {
+                    rem -= T - Rr;
+                    Rr++;
+                }
+                const int Cc = Rr + rem;
+                const int r = t0 + 8 * Rr + g;
+                const int cg = t0 + 8 * Cc + g;
+                const int ca = t0 + 8 * Cc + 2 * t4;
+                double accr[2], acci[2];
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int c = ca + e;
+                    double2 w = make_double2(0.0, 0.0);
+                    if (r < b && c < b && r <= c) w = Ws[r * LP_LD + c];
+                    accr[e] = w.x;
+                    acci[e] = w.y;
+                }
+#pragma unroll
+                for (int k0 = 0; k0 < LP_SUB; k0 += 4) {
+                    const int q = k0 + t4;
+                    double2 u = make_double2(0.0, 0.0), v = make_double2(0.0, 0.0);
+                    if (q < nq && r < b) u = Ws[(s0 + q) * LP_LD + r];  // U(q, r)
+                    if (q < nq && cg < b) v = Wu[q * LDL_NB + cg];      // Wun(q, c)
+                    lp_mma(accr[0], accr[1], -u.x, v.x);
+                    lp_mma(accr[0], accr[1], -u.y, v.y);
+                    lp_mma(acci[0], acci[1], -u.x, v.y);
+                    lp_mma(acci[0], acci[1], u.y, v.x);
+                }
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int c = ca + e;
+                    if (r < b && c < b && r <= c) Ws[r * LP_LD + c] = make_double2(accr[e], acci[e]);
+                }
+            }
+            if (wp == 0) {
+                __syncwarp();
+                eliminate(t0);
+            }
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
+        const int r = e & 63, c = e >> 6;
+        if (r < c && c < b) {
+            const double2 v = Ws[r * LP_LD + c];
+            A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld] = cd{v.x, v.y};
+        }
+    }
+}
+
+// T(s, C): U(s, C) = invD L_ss^-1 W(s, C) for the 64 columns of tile
+// (s, C), L_ss = U_ss^H unit lower, on the FP64 tensor cores by 8-row
+// blocks: with X_b = L_bb^-1 (the inverse of the b-th 8 x 8 diagonal block
+// of L) and the blocks L_ab below it,
+//     Wun_b = X_b W_b,   W_a -= L_ab Wun_b  (a > b),   b = 0..7,
+// which is the substitution of src/linalg.f90:384-389 for eight rows at a
+// time.  Each warp owns eight columns and runs the whole recurrence on them
+// (no barrier between the blocks); the eight X_b are formed first, one per
+// warp, by substitution on the identity.
+constexpr int LT_WP = 66;  // pitch (double2) of the working tile: fragment loads conflict-free
+constexpr size_t LP_SMEM_T = (size_t)(LDL_NB * LT_WP + 2016 + 8 * 64 + LDL_NB) * sizeof(double2);
+
+__device__ __forceinline__ int lt_li(int r, int q) { return r * (r - 1) / 2 + q; }  // packed strict lower, q < r
+
+__device__ void lp_trsm(cd* __restrict__ A, int ld, int n, int s, int C, const cd* __restrict__ invD, double2* sm)
+{
+    double2* Wt = sm;                      // Wt[q * LT_WP + c]: the tile, then Wun
+    double2* Lp = Wt + LDL_NB * LT_WP;     // L(r, q) = conj(U(q, r)), q < r, packed
+    double2* Xb = Lp + 2016;               // X_b(i, j) at Xb[b * 64 + i * 8 + j]
+    double2* ids = Xb + 8 * 64;            // invD of the panel
+    const int p0 = s * LDL_NB, b = min(LDL_NB, n - p0);
+    const int cb = C * LDL_NB, wd = min(LDL_NB, n - cb);
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    const int g = lane >> 2, t4 = lane & 3;
+    for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
+        const int q = e & 63, c = e >> 6;
+        const bool in = q < b && c < wd;
+        cp_async16(Wt + q * LT_WP + c, in ? (const void*)(A + (size_t)(p0 + q) + (size_t)(cb + c) * ld) : (const void*)A,
+                   in ? 16 : 0);
+    }
+    cp_async_commit();
+    for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
+        const int q = e & 63, r = e >> 6;
+        if (q < r) {
+            double2 v = make_double2(0.0, 0.0);
+            if (r < b) {
+                v = lp_ldcg(A + (size_t)(p0 + q) + (size_t)(p0 + r) * ld);
+                v.y = -v.y;
+            }
+            Lp[lt_li(r, q)] = v;
+        }
+    }
+    if (tid < LDL_NB) ids[tid] = tid < b ? lp_ldcg(invD + p0 + tid) : make_double2(0.0, 0.0);
+    __syncthreads();
+    // X_wp = L_bb^-1 for block bb = wp: lane j < 8 holds column j
+    {
+        const int bb = wp, j = lane;
+        cd x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = cd{(i == j) ? 1.0 : 0.0, 0.0};
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+#pragma unroll
+            for (int r = q + 1; r < 8; r++) {
+                const double2 l = Lp[lt_li(8 * bb + r, 8 * bb + q)];
+                x[r] = cfms(cd{l.x, l.y}, x[q], x[r]);
+            }
+        if (j < 8)
+#pragma unroll
+            for (int i = 0; i < 8; i++) Xb[bb * 64 + i * 8 + j] = make_double2(x[i].x, x[i].y);
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    // the recurrence on this warp's eight columns
+    const int c0 = 8 * wp;
+#pragma unroll
+    for (int bk = 0; bk < 8; bk++) {
+        // Wun_b = X_b W_b
+        double wr[2] = {0.0, 0.0}, wi[2] = {0.0, 0.0};
+#pragma unroll
+        for (int k0 = 0; k0 < 8; k0 += 4) {
+            const double2 xa = Xb[bk * 64 + g * 8 + k0 + t4];         // X_b(g, k)
+            const double2 wv = Wt[(8 * bk + k0 + t4) * LT_WP + c0 + g];  // W(k, c)
+            lp_mma(wr[0], wr[1], xa.x, wv.x);
+            lp_mma(wr[0], wr[1], -xa.y, wv.y);
+            lp_mma(wi[0], wi[1], xa.x, wv.y);
+            lp_mma(wi[0], wi[1], xa.y, wv.x);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int e = 0; e < 2; e++) Wt[(8 * bk + g) * LT_WP + c0 + 2 * t4 + e] = make_double2(wr[e], wi[e]);
+        __syncwarp();
+        // W_a -= L_ab Wun_b for the blocks a below
+        double2 un[2];
+#pragma unroll
+        for (int k0 = 0; k0 < 8; k0 += 4) un[k0 / 4] = Wt[(8 * bk + k0 + t4) * LT_WP + c0 + g];  // Wun(k, c)
+#pragma unroll
+        for (int a = bk + 1; a < 8; a++) {
+            double ar[2], ai[2];
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const double2 o = Wt[(8 * a + g) * LT_WP + c0 + 2 * t4 + e];
+                ar[e] = o.x;
+                ai[e] = o.y;
+            }
+#pragma unroll
+            for (int k0 = 0; k0 < 8; k0 += 4) {
+                const double2 l = Lp[lt_li(8 * a + g, 8 * bk + k0 + t4)];  // L(r, k)
+                const double2 u = un[k0 / 4];
+                lp_mma(ar[0], ar[1], -l.x, u.x);
+                lp_mma(ar[0], ar[1], l.y, u.y);
+                lp_mma(ai[0], ai[1], -l.x, u.y);
+                lp_mma(ai[0], ai[1], -l.y, u.x);
+            }
+#pragma unroll
+            for (int e = 0; e < 2; e++) Wt[(8 * a + g) * LT_WP + c0 + 2 * t4 + e] = make_double2(ar[e], ai[e]);
+        }
+        __syncwarp();
+    }
+    // U = invD Wun
+    for (int e = lane; e < LDL_NB * 8; e += 32) {
+        const int q = e & 63, c = c0 + (e >> 6);
+        if (q < b && c < wd) {
+            const double2 v = Wt[q * LT_WP + c], d = ids[q];
+            A[(size_t)(p0 + q) + (size_t)(cb + c) * ld] = cmul(cd{v.x, v.y}, cd{d.x, d.y});
+        }
+    }
+}
+
+// B(s, R, C): W(r, c) -= sum_q conj(U(q, r)) d_q U(q, c) over the 64 x 64
+// tile, r <= c on a diagonal tile (its diagonal in dw).  Eight warps as
+// 2 x 4, each a 32 x 16 complex sub-tile of 8 x 8 mma tiles; the tile's
+// old values are the accumulators' initial values (the minus sign is folded
+// into the operand -d U(q, c)), so a product is accumulated straight onto
+// them; U(s, R) and U(s, C) stream through three cp.async stages of 16 k
+// rows.  m consecutive panels s..s+m-1 (whose rows are contiguous) are
+// applied in one pass when they are all ready: a rank-64m update, the
+// tile read and written once.
+__device__ void lp_update(cd* __restrict__ A, int ld, int n, int s, int m, int R, int C, cd* __restrict__ dw,
+                          double2* sm)
+{
+    constexpr int MT = 4, NT = 2;
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    const int wr = wp >> 2, wc = wp & 3;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int p0 = s * LDL_NB, b = min(m * LDL_NB, n - p0);
+    const int rb = R * LDL_NB, cb = C * LDL_NB;
+    const bool dtile = (R == C);
+    double2* dp = sm + LP_ST * LP_KC * 2 * LP_P;  // pivots d_q of panels s..s+m-1
+    for (int q = tid; q < m * LDL_NB; q += 256) dp[q] = q < b ? lp_ldcg(dw + p0 + q) : make_double2(0.0, 0.0);
+    // a warp whose sub-tile lies wholly below the diagonal has nothing to do
+    const bool wact = !dtile || (wr * 32 <= wc * 16 + 15);
+    auto stage = [&](int ch, int buf) {
+        const int k0 = ch * LP_KC;
+        double2* Us = sm + buf * LP_KC * 2 * LP_P;
+        double2* Vs = Us + LP_KC * LP_P;
+#pragma unroll
+        for (int e = tid; e < LP_KC * LDL_NB; e += 256) {
+            const int q = e % LP_KC, mm = e / LP_KC;
+            const bool kq = k0 + q < b;
+            const int r = rb + mm, c = cb + mm;
+            const bool ku = kq && r < n, kv = kq && c < n;
+            cp_async16(Us + q * LP_P + mm, ku ? (const void*)(A + (size_t)(p0 + k0 + q) + (size_t)r * ld) : (const void*)A,
+                       ku ? 16 : 0);
+            cp_async16(Vs + q * LP_P + mm, kv ? (const void*)(A + (size_t)(p0 + k0 + q) + (size_t)c * ld) : (const void*)A,
+                       kv ? 16 : 0);
+        }
+        cp_async_commit();
+    };
+    const int nch = (b + LP_KC - 1) / LP_KC;
+    stage(0, 0);
+    if (nch > 1) stage(1, 1);
+    double accr[MT][NT][2], acci[MT][NT][2];
+#pragma unroll
+    for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+        for (int nt = 0; nt < NT; nt++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int r = rb + (wr * MT + mt) * 8 + g;
+                const int c = cb + (wc * NT + nt) * 8 + 2 * t4 + e;
+                double2 o = make_double2(0.0, 0.0);
+                if (r < n && c < n && r <= c) {
+                    if (r == c) {
+                        o = lp_ldcg(dw + c);
+                        o.y = -o.y;  // dw keeps the conjugate of the upper-triangle value
+                    } else {
+                        o = lp_ldcg(A + (size_t)r + (size_t)c * ld);
+                    }
+                }
+                accr[mt][nt][e] = o.x;
+                acci[mt][nt][e] = o.y;
+            }
+    for (int ch = 0; ch < nch; ch++) {
+        if (ch + 2 < nch) {
+            __syncthreads();  // buffer (ch + 2) % 3 was read in step ch - 1
+            stage(ch + 2, (ch + 2) % LP_ST);
+            cp_async_wait<2>();
+        } else if (ch + 1 < nch) {
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        if (wact) {
+            const double2* Us = sm + (ch % LP_ST) * LP_KC * 2 * LP_P;
+            const double2* Vs = Us + LP_KC * LP_P;
+#pragma unroll
+            for (int kk = 0; kk < LP_KC; kk += 4) {
+                const double2 d = dp[ch * LP_KC + kk + t4];
+                double2 a[MT];
+                double vr[NT], vi[NT];
+#pragma unroll
+                for (int mt = 0; mt < MT; mt++) a[mt] = Us[(kk + t4) * LP_P + (wr * MT + mt) * 8 + g];
+#pragma unroll
+                for (int nt = 0; nt < NT; nt++) {
+                    const double2 v = Vs[(kk + t4) * LP_P + (wc * NT + nt) * 8 + g];
+                    // -(d v): the unscaled row, negated
+                    vr[nt] = -fma(v.x, d.x, -v.y * d.y);
+                    vi[nt] = -fma(v.x, d.y, v.y * d.x);
+                }
+#pragma unroll
+                for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+                    for (int nt = 0; nt < NT; nt++) {
+                        lp_mma(accr[mt][nt][0], accr[mt][nt][1], a[mt].x, vr[nt]);
+                        lp_mma(accr[mt][nt][0], accr[mt][nt][1], a[mt].y, vi[nt]);
+                        lp_mma(acci[mt][nt][0], acci[mt][nt][1], a[mt].x, vi[nt]);
+                        lp_mma(acci[mt][nt][0], acci[mt][nt][1], -a[mt].y, vr[nt]);
+                    }
+            }
+        }
+    }
+#pragma unroll
+    for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+        for (int nt = 0; nt < NT; nt++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int r = rb + (wr * MT + mt) * 8 + g;
+                const int c = cb + (wc * NT + nt) * 8 + 2 * t4 + e;
+                if (r >= n || c >= n || c < r) continue;
+                if (c == r)
+                    dw[c] = cd{accr[mt][nt][e], -acci[mt][nt][e]};
+                else
+                    A[(size_t)r + (size_t)c * ld] = cd{accr[mt][nt][e], acci[mt][nt][e]};
+            }
+}
+
+constexpr size_t lp_max(size_t a, size_t b) { return a > b ? a : b; }
+constexpr size_t LP_SMEM = lp_max(LP_SMEM_B, lp_max(LP_SMEM_D, LP_SMEM_T));
+
+struct LpArgs {
+    cd* A;
+    int ld, n, np;
+    const unsigned* tasks;  // the list of the CTAs other than the chain CTA
+    int ntasks;
+    unsigned* cnt;          // tile counters
+    unsigned* ctl;          // [0] next list index, [1] abort word, [2] trace records, [3] chain CTA's SM + 1
+    cd* dw;
+    cd* invD;
+    int* status;
+    const int* limitp;      // poll limit of the bounded waits
+    unsigned long long* trace;  // optional: per task (code | cta << 32 | panels << 48, start, ready, done)
+};
+
+__device__ __forceinline__ unsigned long long lp_clock()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Thread 0: wait until cnt[ix[i]] >= need[i] for the k (<= 3) conditions,
+// polling them together.  False when this CTA must stop.
+__device__ __forceinline__ bool lp_wait_all(const LpArgs& a, const long long (&ix)[3], const unsigned (&need)[3],
+                                            int k, int limit)
+{
+    int spins = 0;
+    for (;;) {
+        unsigned v[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) v[i] = (i < k) ? lp_ld_acquire(a.cnt + ix[i]) : 0u;
+        bool ok = true;
+#pragma unroll
+        for (int i = 0; i < 3; i++) ok = ok && (i >= k || v[i] >= need[i]);
+        if (ok) return true;
+        if (++spins > limit || *((volatile unsigned*)(a.ctl + 1)) != 0u) {
+            atomicExch(a.status + ST_SOLVE_TIMEOUT, 1);
+            atomicExch(a.ctl + 1, 1u);
+            return false;
+        }
+        __nanosleep(32);
+    }
+}
+
+__device__ __forceinline__ void lp_trace(const LpArgs& a, unsigned code, int m, unsigned long long t0,
+                                         unsigned long long t1)
+{
+    if (!a.trace) return;
+    const unsigned long long t2 = lp_clock();
+    const unsigned i = atomicAdd(a.ctl + 2, 1u);
+    unsigned long long* r = a.trace + 4 * (size_t)i;
+    r[0] = (unsigned long long)code | (unsigned long long)blockIdx.x << 32 | (unsigned long long)m << 48;
+    r[1] = t0;
+    r[2] = t1;
+    r[3] = t2;
+}
+
+// One task, all threads.  Thread 0 has checked the dependencies; on return
+// the task's stores are done (a barrier follows).  m: panels of an update.
+template <bool CPLX>
+__device__ __forceinline__ void lp_exec(const LpArgs& a, unsigned type, int s, int m, int R, int C, double2* sm)
+{
+    if (type == LP_D)
+        lp_diag<CPLX>(a.A, a.ld, a.n, s, a.dw, a.invD, a.status, sm);
+    else if (type == LP_T)
+        lp_trsm(a.A, a.ld, a.n, s, C, a.invD, sm);
+    else
+        lp_update(a.A, a.ld, a.n, s, m, R, C, a.dw, sm);
+}
+
+// After the task's barrier: thread 0 publishes the tile's new count.  The
+// barrier orders every thread's stores before the gpu-scope release.
+__device__ __forceinline__ void lp_publish(const LpArgs& a, long long ix, unsigned v)
+{
+    if (threadIdx.x == 0) lp_st_release(a.cnt + ix, v);
+}
+
+// CTA 0 runs the critical chain, per panel s: D(s), then T(s, s+1) and
+// B(s, s+1, s+1), which D(s+1) needs; D(s) is published before the other
+// two so that the panel rows of the other tiles start at once.  The other
+// CTAs take every remaining task from the list, each when it is free.  An update B(s, R, C)
+// whose tile already carries more than s panels (applied by an earlier
+// merged update) does nothing; otherwise it also applies the following
+// panels s+1.. (up to LP_MERGE in all, below R) whose panel rows of R and
+// C are already final.
+template <bool CPLX>
+__global__ void __launch_bounds__(256, 2) k_ldl_persist(LpArgs a)
+{
+    extern __shared__ double2 lsm[];
+    __shared__ unsigned s_next;
+    __shared__ int s_go, s_m;
+    const int tid = threadIdx.x;
+    const int limit = *((const volatile int*)a.limitp);
+    // the chain CTA has its SM to itself: it publishes its SM, and the CTA
+    // sharing that SM takes no tasks
+    if (tid == 0) {
+        unsigned smid;
+        asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+        int go = 1;
+        if (blockIdx.x == 0) {
+            lp_st_release(a.ctl + 3, smid + 1);
+        } else {
+            int spins = 0;
+            unsigned v;
+            while ((v = lp_ld_acquire(a.ctl + 3)) == 0u) {
+                if (++spins > limit || *((volatile unsigned*)(a.ctl + 1)) != 0u) {
+                    atomicExch(a.status + ST_SOLVE_TIMEOUT, 1);
+                    atomicExch(a.ctl + 1, 1u);
+                    break;
+                }
+                __nanosleep(32);
+            }
+            go = (v != 0u && v != smid + 1);
+        }
+        s_go = go;
+    }
+    __syncthreads();
+    if (!s_go) return;
+    if (blockIdx.x == 0) {
+        for (int s = 0; s < a.np; s++) {
+            for (int step = 0; step < 3; step++) {
+                if (step > 0 && s + 1 >= a.np) break;
+                const unsigned type = (step == 0) ? LP_D : (step == 1) ? LP_T : LP_B;
+                const int R = (step == 2) ? s + 1 : s, C = (step == 0) ? s : s + 1;
+                const long long tix = lp_tix(R, C);
+                unsigned long long t0 = 0, t1 = 0;
+                if (tid == 0) {
+                    if (a.trace) t0 = lp_clock();
+                    long long ix[3] = {tix, 0, 0};
+                    unsigned need[3] = {(unsigned)s, 0u, 0u};
+                    int go = lp_wait_all(a, ix, need, 1, limit) ? 1 : 0;
+                    // an update already applied by a merged update is skipped
+                    if (go && step == 2 && lp_ld_acquire(a.cnt + tix) > (unsigned)s) go = 2;
+                    s_go = go;
+                    if (a.trace) t1 = lp_clock();
+                }
+                __syncthreads();
+                const int go = s_go;
+                if (!go) return;
+                if (go == 1) {
+                    lp_exec<CPLX>(a, type, s, 1, R, C, lsm);
+                    __syncthreads();
+                    lp_publish(a, tix, (unsigned)s + 1);
+                }
+                if (tid == 0) lp_trace(a, lp_code(type, s, R, C), go == 1 ? 1 : 0, t0, t1);
+                __syncthreads();  // s_go is rewritten by the next step
+            }
+        }
+        return;
+    }
+    for (;;) {
+        unsigned long long t0 = 0, t1 = 0;
+        if (tid == 0) {
+            if (a.trace) t0 = lp_clock();
+            // the next task in list order, taken when this CTA is free (a
+            // task fetched earlier could wait behind a long update)
+            unsigned task = LP_NONE;
+            if (*((volatile unsigned*)(a.ctl + 1)) == 0u) {
+                const unsigned i = atomicAdd(a.ctl, 1u);
+                if (i < (unsigned)a.ntasks) task = __ldg(a.tasks + i);
+            }
+            int go = 0, m = 1;
+            if (task != LP_NONE) {
+                const unsigned type = task >> 30;
+                const int s = (task >> 20) & 1023, R = (task >> 10) & 1023, C = task & 1023;
+                long long ix[3] = {0, 0, 0};
+                unsigned need[3] = {0u, 0u, 0u};
+                int k = 0;
+                if (type == LP_D) {
+                    ix[0] = lp_tix(s, s), need[0] = (unsigned)s, k = 1;
+                } else if (type == LP_T) {
+                    ix[0] = lp_tix(s, s), need[0] = (unsigned)s + 1;
+                    ix[1] = lp_tix(s, C), need[1] = (unsigned)s, k = 2;
+                } else {
+                    ix[0] = lp_tix(R, C), need[0] = (unsigned)s;
+                    ix[1] = lp_tix(s, R), need[1] = (unsigned)s + 1;
+                    ix[2] = lp_tix(s, C), need[2] = (unsigned)s + 1;
+                    k = (R == C) ? 2 : 3;
+                }
+                go = lp_wait_all(a, ix, need, k, limit) ? 1 : 0;
+                if (go && type == LP_B) {
+                    if (lp_ld_acquire(a.cnt + ix[0]) > (unsigned)s) {
+                        go = 2;  // applied already by a merged update
+                    } else {
+                        // following panels whose rows of R and C are final
+                        unsigned fr[LP_MERGE - 1], fc[LP_MERGE - 1];
+#pragma unroll
+                        for (int j = 1; j < LP_MERGE; j++) {
+                            const bool in = s + j < R;
+                            fr[j - 1] = in ? lp_ld_acquire(a.cnt + lp_tix(s + j, R)) : 0u;
+                            fc[j - 1] = (in && R != C) ? lp_ld_acquire(a.cnt + lp_tix(s + j, C)) : 0u;
+                        }
+#pragma unroll
+                        for (int j = 1; j < LP_MERGE; j++) {
+                            const unsigned want = (unsigned)(s + j) + 1;
+                            if (m == j && s + j < R && fr[j - 1] >= want && (R == C || fc[j - 1] >= want)) m = j + 1;
+                        }
+                    }
+                }
+                if (!go) task = LP_NONE;
+            }
+            s_next = task;
+            s_go = go;
+            s_m = m;
+            if (a.trace) t1 = lp_clock();
+        }
+        __syncthreads();
+        const unsigned task = s_next;
+        const int go = s_go, m = s_m;
+        if (task == LP_NONE) return;
+        const unsigned type = task >> 30;
+        const int s = (task >> 20) & 1023, R = (task >> 10) & 1023, C = task & 1023;
+        if (go == 1) {
+            lp_exec<CPLX>(a, type, s, m, R, C, lsm);
+            __syncthreads();
+            lp_publish(a, (type == LP_B) ? lp_tix(R, C) : lp_tix(s, (type == LP_D) ? s : C), (unsigned)(s + m));
+        }
+        if (tid == 0) lp_trace(a, task, go == 1 ? m : 0, t0, t1);
+        __syncthreads();  // s_next, s_go, s_m are rewritten by the next task
+    }
+}
+
+static bool g_lp_attr = false;
+
+// Grid of the persistent kernel (co-resident CTAs), 0 if unavailable.
+int ldlp_grid(Ctx& c)
+{
+    if (!g_lp_attr) {
+        if (cudaFuncSetAttribute(k_ldl_persist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LP_SMEM) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(k_ldl_persist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LP_SMEM) !=
+                cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        g_lp_attr = true;
+    }
+    if (c.lp_grid > 0) return c.lp_grid;
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ldl_persist<false>, 256, LP_SMEM) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c.dev);
+    if (!coop || per_sm < 1) return 0;
+    c.lp_grid = per_sm * sms;
+    return c.lp_grid;
+}
+
+// The task list of an n-row factorisation in device memory (owned by the
+// caller, freed with cudaFree; at least one entry); *count receives its
+// length (0 when the chain CTA does everything).
+int ldlp_tasks(Ctx& c, int n, unsigned** tasks, int* count)
+{
+    const int grid = ldlp_grid(c);
+    if (grid <= 0) return -1;
+    const int np = (n + LDL_NB - 1) / LDL_NB;
+    if (np > 1023) return -1;
+    const std::vector<unsigned> list = lp_schedule(np, grid, LpCost());
+    unsigned* d = nullptr;
+    if (cudaMalloc(&d, std::max<size_t>(1, list.size()) * sizeof(unsigned)) != cudaSuccess) {
+        cudaGetLastError();
+        return -3;
+    }
+    if (!list.empty() &&
+        cudaMemcpy(d, list.data(), list.size() * sizeof(unsigned), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(d);
+        return -2;
+    }
+    *tasks = d;
+    *count = (int)list.size();
+    return 0;
+}
+
+// Number of tasks of an n-row factorisation, the chain's included.
+long long ldlp_task_total(int n)
+{
+    const long long np = (n + LDL_NB - 1) / LDL_NB;
+    return np + np * (np - 1) / 2 + (np - 1) * np * (np + 1) / 6;
+}
+
+// Tile counters and the control words (next task, abort word, trace
+// records, the chain CTA's SM) for np panels.
+int ldlp_reserve(Ctx& c, int np)
+{
+    const size_t need = (size_t)np * (np + 1) / 2 + 4;
+    if (c.lp_cap >= need) return 0;
+    if (c.lp_cnt) cudaFree(c.lp_cnt);
+    c.lp_cnt = nullptr;
+    c.lp_cap = 0;
+    if (cudaMalloc(&c.lp_cnt, need * sizeof(unsigned)) != cudaSuccess) {
+        cudaGetLastError();
+        return -3;
+    }
+    c.lp_cap = need;
+    return 0;
+}
+
+// Queue one persistent factorisation of rows 0..n-1 (the working upper
+// triangle and dw already initialised by k_ldl_mirror); trace (device,
+// 4 x ldlp_task_total(n) values) may be null.
+void ldlp_enqueue(Ctx& c, int n, const unsigned* tasks, int ntasks, unsigned long long* trace)
+{
+    const int np = (n + LDL_NB - 1) / LDL_NB;
+    const size_t ntile = (size_t)np * (np + 1) / 2;
+    cudaMemsetAsync(c.lp_cnt, 0, (ntile + 4) * sizeof(unsigned), c.stream);
+    LpArgs a;
+    a.A = c.F;
+    a.ld = c.ld;
+    a.n = n;
+    a.np = np;
+    a.tasks = tasks;
+    a.ntasks = ntasks;
+    a.cnt = c.lp_cnt;
+    a.ctl = c.lp_cnt + ntile;
+    a.dw = c.dw;
+    a.invD = c.invD;
+    a.status = c.status;
+    a.limitp = c.counters + 3;
+    a.trace = trace;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.gridDim = dim3(std::min(c.lp_grid, 1 + ntasks));
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = LP_SMEM;
+    cfg.stream = c.stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (c.pivot_mode)
+        cudaLaunchKernelEx(&cfg, k_ldl_persist<true>, a);
+    else
+        cudaLaunchKernelEx(&cfg, k_ldl_persist<false>, a);
+    c.launches++;
+}
+
+}  // namespace ecg
+
+// Host-only diagnostic: every task of the persistent factorisation of n
+// rows for a grid of `workers` CTAs in the scheduler's start order (the
+// chain CTA's tasks included; the kernel's list is this order without
+// them).  No GPU needed.
+extern "C" int ecg_ldl_schedule(int n, int workers, unsigned* out, long long cap, long long* count)
+{
+    using namespace ecg;
+    if (n < 1 || workers < 1 || !count) return -1;
+    const int np = (n + LDL_NB - 1) / LDL_NB;
+    if (np > 1023) return -1;
+    std::vector<unsigned> full;
+    lp_schedule(np, workers, LpCost(), &full);
+    *count = (long long)full.size();
+    if (out && cap >= (long long)full.size()) std::copy(full.begin(), full.end(), out);
+    return 0;
+}

@@ -61,6 +61,9 @@ PROTOTYPES = {
     "ecg_get_tuning": (C.c_int, [_vp, _ip, _ip, _ip, _dp]),
     "ecg_set_pivot_mode": (C.c_int, [_vp, C.c_int]),
     "ecg_set_wait_limit": (C.c_int, [_vp, C.c_int]),
+    "ecg_set_factor_mode": (C.c_int, [_vp, C.c_int]),
+    "ecg_factor_trace": (C.c_int, [_vp, C.c_int, C.c_void_p, C.c_longlong, C.POINTER(C.c_longlong)]),
+    "ecg_ldl_schedule": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_longlong, C.POINTER(C.c_longlong)]),
     "ecg_io_bytes": (C.c_int, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "ecg_probe_fp64_peak": (C.c_int, [C.c_int, _dp]),
     "ecg_probe_fp64_tensor_peak": (C.c_int, [C.c_int, _dp]),

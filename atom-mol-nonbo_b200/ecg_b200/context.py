@@ -405,8 +405,23 @@ class Context:
         _check(self.lib.ecg_set_pivot_mode(self.h, int(mode)), "ecg_set_pivot_mode")
 
     def set_wait_limit(self, polls):
-        """Poll limit of the solves' bounded device waits (< 0: default)."""
+        """Poll limit of the bounded device waits (< 0: default)."""
         _check(self.lib.ecg_set_wait_limit(self.h, int(polls)), "ecg_set_wait_limit")
+
+    def set_factor_mode(self, mode):
+        """Whole-matrix LDL^H: 0 persistent tile kernel (default), 1 one launch per panel step."""
+        _check(self.lib.ecg_set_factor_mode(self.h, int(mode)), "ecg_set_factor_mode")
+
+    def factor_trace(self, n):
+        """One traced persistent factorisation of the current matrix
+        (ecg_factor_trace): an (records, 4) uint64 array."""
+        cnt = C.c_longlong()
+        np_ = (n + 63) // 64
+        total = np_ + np_ * (np_ - 1) // 2 + (np_ - 1) * np_ * (np_ + 1) // 6
+        out = np.zeros((total, 4), dtype=np.uint64)
+        _check(self.lib.ecg_factor_trace(self.h, int(n), C.c_void_p(out.ctypes.data), out.size, C.byref(cnt)),
+               "ecg_factor_trace")
+        return out[:cnt.value]
 
     def io_bytes(self):
         a, b = C.c_longlong(), C.c_longlong()

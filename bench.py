@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--only-expc", type=int, default=0, help="time only the expectation-value pass (profiling)")
     ap.add_argument("--lam", type=float, default=None,
                     help="use this lambda~ instead of the stored one or a search (profiling runs)")
+    ap.add_argument("--factor-mode", type=int, default=0,
+                    help="whole-matrix LDL^H: 0 persistent tile kernel (default), 1 one launch per panel step")
     ap.add_argument("--ref-max-iter", type=int, default=None,
                     help="MaxIter of the reference arm's GHEPIIS (default 20, the reference's)")
     return ap.parse_args()
@@ -230,6 +232,7 @@ def run_ours(args, dist):
     pairs = K * (K + 1) // 2
     fx = load_fixture(K) if dist.rank == 0 else None
     ctx = Context(sysm, K, max_nfo=K if args.plain_steps > 0 else 0, device=dev)
+    ctx.set_factor_mode(args.factor_mode)
     ctx.set_params(params)
     if args.lam is not None:
         lam = args.lam
@@ -549,6 +552,7 @@ def run_large(args, dev, rank):
                                         row_scale=synth.reduced_mass_scale(sysm.masses))
         e_floor = synth.SYSTEMS[cfg["system"]]["e_floor"]
         with Context(sysm, K, device=dev) as ctx:
+            ctx.set_factor_mode(args.factor_mode)
             ctx.set_params(params)
             ctx.set_vectors(K, last_eigvec=np.ones(K, dtype=np.complex128))
             E0, err0, it0 = ctx.energy_ia(1, K, e_floor, -1e-12, max_iter=300, specif_norm=0)

@@ -319,13 +319,42 @@ int ecg_get_tuning(ecg_ctx* ctx, int* pair_shape, int* adjoint_shape, int* cand_
  * EIGVAL_TOLERANCE = 1e-12 mode 1 returns ErrorCode 2 where the reference
  * does and mode 0 converges.  Changing the mode discards the factor. */
 int ecg_set_pivot_mode(ecg_ctx* ctx, int mode);
-/* Poll limit of the bounded device waits in the context's triangular
- * solves (GHEPIIS and the batched candidates): every wait on another CTA's
- * panel gives up after `polls` polls (about 64 ns each), records the
- * timeout and the call returns ECG_ECUDA with the context still usable.
- * polls < 0 restores the default (2^22).  No counterpart in the reference:
- * a diagnostic that lets a test make a wait run out without a fault. */
+/* How the context factorises a whole matrix (LDLHF with m = 1, the first
+ * step of every EnergyIA/IB(0, K) and of the 'G' path): mode 0 (default)
+ * one persistent cooperative kernel over 64 x 64 tiles whose CTAs take
+ * the diagonal eliminations, panel rows and trailing updates from a
+ * critical-path-ordered task list; mode 1 one launch per panel step
+ * (diagonal block, panel rows, trailing update on a second stream).  Both
+ * give the same factor up to rounding.  No counterpart in the reference
+ * (its LDLHF is one code path); kept for comparison and measurement. */
+int ecg_set_factor_mode(ecg_ctx* ctx, int mode);
+/* Factorise rows 1..n of the context's current matrix (the lower triangle
+ * that ecg_compute_mat_elem / ecg_ghepiis leave: H - lambda~ S) once with
+ * the persistent kernel, outside any graph, recording per task: the task
+ * code (as ecg_ldl_schedule) | CTA << 32 | panels applied << 48 (0: found
+ * already applied), and the GPU's globaltimer (ns) when the CTA began
+ * waiting for the task's tiles, when they were ready and when the task was
+ * published.  *count receives the number of records; records (capacity cap
+ * values, 4 per record) is filled when large enough.  The factor is left as
+ * GHEPIIS's factorisation leaves it.  No counterpart in the reference: a
+ * measurement aid. */
+int ecg_factor_trace(ecg_ctx* ctx, int n, unsigned long long* records, long long cap, long long* count);
+/* Poll limit of the bounded device waits of the context (the triangular
+ * solves of GHEPIIS and of the batched candidates, and the tile waits of
+ * the persistent factorisation): every wait on another CTA's work gives up
+ * after `polls` polls, records the timeout and the call returns ECG_ECUDA
+ * with the context still usable.  polls < 0 restores the default (2^22).
+ * No counterpart in the reference: a diagnostic that lets a test make a
+ * wait run out without a fault. */
 int ecg_set_wait_limit(ecg_ctx* ctx, int polls);
+/* The task list of the persistent factorisation of n rows for `workers`
+ * CTAs, on the host (no GPU needed): codes type << 30 | s << 20 | R << 10 |
+ * C, type 0 = D(s) (diagonal tile s), 1 = T(s, C) (panel rows of tile
+ * (s, C)), 2 = B(s, R, C) (update of tile (R, C) by panel s), 64-row
+ * tiles.  *count receives the length; out (capacity cap) is filled when it
+ * is large enough.  No counterpart in the reference: exposes the task order
+ * to tests. */
+int ecg_ldl_schedule(int n, int workers, unsigned* out, long long cap, long long* count);
 /* Bytes this context has copied host->device and device->host so far. */
 int ecg_io_bytes(ecg_ctx* ctx, long long* h2d, long long* d2h);
 /* The fused adjoint gradient of ecg_energy_ib_adjoint, for callers that

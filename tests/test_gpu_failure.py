@@ -15,7 +15,12 @@ pytestmark = pytest.mark.gpu
 ECG_ECUDA = -2
 
 
-def test_ghepiis_wait_timeout_is_reported_and_the_context_recovers():
+def test_factorisation_wait_timeout_is_reported_and_the_context_recovers():
+    """EnergyIA(1, K) factorises the whole matrix with the persistent tile
+    kernel: with the poll limit at 0 the first task that finds a tile it
+    depends on unfinished gives up, every CTA stops taking tasks, and the
+    call reports ECG_ECUDA; the factorisation is deterministic, so the next
+    call reproduces the first result bit for bit."""
     K = 400
     sysm, params, lam, _ = problem(1, K)
     ones = np.ones(K, dtype=np.complex128)
@@ -31,6 +36,31 @@ def test_ghepiis_wait_timeout_is_reported_and_the_context_recovers():
         ctx.set_wait_limit(-1)
         ctx.set_vectors(K, last_eigvec=ones)
         E1, err1, it1 = ctx.energy_ia(1, K, lam, 1e-12)
+    print(f"E before {E0:.15f} after {E1:.15f}")
+    assert (err1, it1) == (err0, it0) and E1 == E0
+
+
+def test_ghepiis_wait_timeout_is_reported_and_the_context_recovers():
+    """EnergyIA(K, K) recomputes row K and extends the existing factor by
+    one row (the bordered LDLHF, no waits), so the bounded waits that run
+    out are those of GHEPIIS's cooperative triangular solves."""
+    K = 400
+    sysm, params, lam, _ = problem(1, K)
+    ones = np.ones(K, dtype=np.complex128)
+    with Context(sysm, K) as ctx:
+        ctx.set_params(params)
+        ctx.set_vectors(K, last_eigvec=ones)
+        ctx.energy_ia(1, K, lam, 1e-12)
+        ctx.set_vectors(K, last_eigvec=ones)
+        E0, err0, it0 = ctx.energy_ia(K, K, lam, 1e-12)
+        ctx.set_wait_limit(0)
+        ctx.set_vectors(K, last_eigvec=ones)
+        with pytest.raises(EcgError) as ei:
+            ctx.energy_ia(K, K, lam, 1e-12)
+        assert ei.value.status == ECG_ECUDA
+        ctx.set_wait_limit(-1)
+        ctx.set_vectors(K, last_eigvec=ones)
+        E1, err1, it1 = ctx.energy_ia(K, K, lam, 1e-12)
     print(f"E before {E0:.15f} after {E1:.15f}")
     assert (err1, it1) == (err0, it0) and E1 == E0
 
