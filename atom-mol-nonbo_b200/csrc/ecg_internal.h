@@ -165,7 +165,8 @@ struct Ctx {
         std::vector<int> key;
         cudaGraphExec_t exec = nullptr;
         long long launches = 0;  // kernel launches one replay performs
-        unsigned* tasks = nullptr;  // task list of a persistent factorisation (ldlp.cu), owned
+        unsigned* tasks = nullptr;  // task lists of a persistent factorisation (ldlp.cu), owned
+        int ntasks = 0;
     };
     long long graph_launches = 0;
     std::vector<LdlGraph> ldl_graphs;
@@ -174,6 +175,7 @@ struct Ctx {
     // persistent factorisation of whole matrices (ldlp.cu)
     int factor_mode = 0;        // 0: persistent kernel for m0 = 0, 1: one launch per panel step
     int lp_grid = 0;            // co-resident CTAs of the persistent kernel (0: not yet known)
+    int lp_sms = 1;             // SMs of the device
     unsigned* lp_cnt = nullptr; // tile counters, then the next-task counter and the abort word
     size_t lp_cap = 0;          // capacity of lp_cnt (unsigned)
     unsigned* lp_direct = nullptr;  // task list of the uncaptured fallback, for lp_direct_n rows

@@ -741,6 +741,7 @@ int ldlh_factor(Ctx& c, int m0, int n)
         g = &c.ldl_graphs.back();
         g->launches = c.graph_launches;
         g->tasks = tasks;
+        g->ntasks = ntasks;
     }
     if (cudaGraphLaunch(g->exec, c.stream) != cudaSuccess) return -2;
     c.launches += g->launches;
@@ -781,7 +782,7 @@ int ldlh_factor_traced(Ctx& c, int n, unsigned long long* out, long long cap, lo
     }
     enqueue_persist(c, n, tasks, ntasks, d);
     unsigned recs = 0;
-    const size_t ntile = (size_t)nb * (nb + 1) / 2;
+    const size_t ntile = (size_t)nb * (nb + 1) / 2;  // trace records at ctl[2], ctl = counters + ntile
     int r = 0;
     if (cudaMemcpyAsync(&recs, c.lp_cnt + ntile + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, c.stream) !=
             cudaSuccess ||

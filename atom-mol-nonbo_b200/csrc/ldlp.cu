@@ -9,8 +9,7 @@
 // (R, C), R <= C, of panel index s:
 //   D(s)        eliminate the diagonal tile (s, s): U_ss, invD, pivots d_s
 //               (written to dw over the consumed working diagonal);
-//   T(s, C)     panel rows of tile (s, C) by substitution with U_ss:
-//               U(s, C) = invD L_ss^-1 W(s, C);
+//   T(s, C)     panel rows of tile (s, C): U(s, C) = invD L_ss^-1 W(s, C);
 //   B(s, R, C)  W(R, C) -= conj(U(s, R))^T diag(d_s) U(s, C), s < R <= C
 //               (the unscaled rows of the reference's recurrence, d U, are
 //               formed in registers from U and d instead of being stored).
@@ -19,17 +18,23 @@
 // tiles carry the counts it needs:
 //   D(s): cnt(s,s) >= s;  T(s,C): cnt(s,s) >= s+1, cnt(s,C) >= s;
 //   B(s,R,C): cnt(s,R) >= s+1, cnt(s,C) >= s+1, cnt(R,C) >= s.
-// The CTAs (all co-resident: cooperative launch) take tasks from a list in
-// a fixed order through one atomic counter.  The list is a topological order
-// of that dependency graph, made on the host by list scheduling on as many
-// simulated workers as the grid has CTAs, always starting the ready task
-// with the longest remaining path (upward rank), so the chain D(s) -> T(s,
-// s+1) -> B(s, s+1, s+1) -> D(s+1) goes first and the trailing updates fill
-// the rest.  Because every task's dependencies come earlier in the list and
-// every CTA is resident, the earliest unfinished task can always proceed:
-// the kernel cannot deadlock.  Waits are still bounded (the poll limit of
-// ecg_set_wait_limit); a CTA that gives up records ST_SOLVE_TIMEOUT and
-// sets the abort word, after which every CTA stops taking tasks.
+// CTA 0, alone on its SM, runs the chain D(s) -> T(s, s+1) -> B(s, s+1,
+// s+1) -> D(s+1) with the diagonal tile kept in shared memory.  The other
+// CTAs (all co-resident: cooperative launch) take every other task from a
+// list in a fixed order through one atomic counter; an update whose next
+// panels are already final applies them too (rank up to 256).  The list is
+// a topological order of the dependency graph, made on the host by list
+// scheduling on as many simulated workers as the grid has CTAs, always
+// starting the ready task with the longest remaining path (upward rank).
+// Because every task's dependencies come earlier in that order (the chain's
+// included) and every CTA is resident, the earliest unfinished task can
+// always proceed: the kernel cannot deadlock.  Waits are still bounded (the
+// poll limit of ecg_set_wait_limit); a CTA that gives up records
+// ST_SOLVE_TIMEOUT and sets the abort word, after which every CTA stops
+// taking tasks.  The kernel's code is kept compact (loops that are not
+// unrolled where unrolling gained nothing): the chain's per-panel loop has
+// to stay in the instruction cache, and a larger form measured D(s) at 42
+// instead of 21 us.
 #include <algorithm>
 #include <queue>
 #include <utility>
@@ -48,7 +53,6 @@ constexpr int LP_LD = LDL_NB + 1;  // pitch of the 64 x 64 shared tiles of D and
 constexpr int LP_SUB = 8;          // sub-panel rows of the diagonal elimination
 constexpr int LP_MERGE = 4;        // most panels one trailing update applies at once
 constexpr size_t LP_SMEM_B = (size_t)(LP_ST * LP_KC * 2 * LP_P + LP_MERGE * LDL_NB) * sizeof(double2);
-constexpr size_t LP_SMEM_D = (size_t)(LDL_NB * LP_LD + LP_SUB * LDL_NB) * sizeof(double2);
 
 __host__ __device__ __forceinline__ unsigned lp_code(unsigned type, int s, int R, int C)
 {
@@ -64,13 +68,14 @@ __host__ __device__ __forceinline__ long long lp_tix(int R, int C) { return (lon
 // two CTAs per SM (globaltimer records of ecg_factor_trace); only their
 // ratios and the resulting priorities matter.
 struct LpCost {
-    double d = 28.0, t = 18.0, b = 24.0, bd = 18.0;
+    double d = 21.0, t = 20.0, b = 24.0, bd = 15.0;
 };
 
-// Tasks of a factorisation with np panels for a grid of P CTAs: the list
-// the CTAs other than the chain CTA take, and (if full is given) every task
-// in the simulated start order, the chain's included.
-static std::vector<unsigned> lp_schedule(int np, int P, const LpCost& cost, std::vector<unsigned>* full = nullptr)
+// Tasks of a factorisation with np panels: the list the P CTAs other than
+// the chain CTA take, and (if full is given) every task in the simulated
+// start order, the chain's included.
+static void lp_schedule(int np, int P, const LpCost& cost, std::vector<unsigned>& list,
+                        std::vector<unsigned>* full = nullptr)
 {
     std::vector<unsigned> code;
     std::vector<long long> idD(np), baseB(np);
@@ -135,18 +140,18 @@ static std::vector<unsigned> lp_schedule(int np, int P, const LpCost& cost, std:
         rank[(size_t)t] = w[(size_t)t] + m;
     }
     // list scheduling: the chain worker runs D(s), T(s, s+1), B(s, s+1,
-    // s+1) in that order, each as soon as it is ready; P - 1 list workers
+    // s+1) in that order, each as soon as it is ready; the P list workers
     // start the ready task of highest rank (earliest created among equals)
     // whenever one of them is free.  `full` receives every task in start
-    // order, the returned list the tasks of the list workers.
-    std::vector<char> chain((size_t)N, 0);
+    // order.
+    std::vector<char> pool((size_t)N, 1);  // 0 chain, 1 list
     std::vector<long long> cseq;
     for (int s = 0; s < np; s++) {
-        chain[(size_t)idD[s]] = 1;
+        pool[(size_t)idD[s]] = 0;
         cseq.push_back(idD[s]);
         if (s + 1 < np) {
             const long long t = idT[(size_t)s * np + s + 1], b = idB(s, s + 1, s + 1);
-            chain[(size_t)t] = chain[(size_t)b] = 1;
+            pool[(size_t)t] = pool[(size_t)b] = 0;
             cseq.push_back(t);
             cseq.push_back(b);
         }
@@ -158,51 +163,45 @@ static std::vector<unsigned> lp_schedule(int np, int P, const LpCost& cost, std:
     std::priority_queue<Item> ready;                                        // (rank, -id)
     std::priority_queue<Item, std::vector<Item>, std::greater<Item>> busy;  // (finish, id)
     for (long long t = 0; t < N; t++)
-        if (npred[(size_t)t] == 0 && !chain[(size_t)t]) ready.push({rank[(size_t)t], -t});
-    std::vector<unsigned> order;
-    order.reserve((size_t)N);
+        if (npred[(size_t)t] == 0 && pool[(size_t)t]) ready.push({rank[(size_t)t], -t});
+    list.clear();
     if (full) {
         full->clear();
         full->reserve((size_t)N);
     }
-    int free_w = std::max(1, P - 1);
-    bool chain_free = true;
+    int free_w[2] = {1, std::max(1, P)};
     size_t ci = 0;
     long long started = 0;
     double now = 0.0;
     while (started < N) {
-        if (chain_free && ci < cseq.size() && npred[(size_t)cseq[ci]] == 0) {
+        if (free_w[0] > 0 && ci < cseq.size() && npred[(size_t)cseq[ci]] == 0) {
             const long long t = cseq[ci];
             if (full) full->push_back(code[(size_t)t]);
             busy.push({now + w[(size_t)t], t});
-            chain_free = false;
+            free_w[0]--;
             started++;
         }
-        while (free_w > 0 && !ready.empty()) {
+        while (free_w[1] > 0 && !ready.empty()) {
             const long long t = -ready.top().second;
             ready.pop();
-            order.push_back(code[(size_t)t]);
+            list.push_back(code[(size_t)t]);
             if (full) full->push_back(code[(size_t)t]);
             busy.push({now + w[(size_t)t], t});
-            free_w--;
+            free_w[1]--;
             started++;
         }
         if (busy.empty()) break;  // cannot happen for a valid graph
         const Item f = busy.top();
         busy.pop();
         now = f.first;
-        if (chain[(size_t)f.second]) {
-            chain_free = true;
-            ci++;
-        } else {
-            free_w++;
-        }
+        const int fp = pool[(size_t)f.second];
+        free_w[fp]++;
+        if (fp == 0) ci++;
         for (long long e = so[(size_t)f.second]; e < so[(size_t)f.second + 1]; e++) {
             const long long q = sl[(size_t)e];
-            if (--npred[(size_t)q] == 0 && !chain[(size_t)q]) ready.push({rank[(size_t)q], -q});
+            if (--npred[(size_t)q] == 0 && pool[(size_t)q]) ready.push({rank[(size_t)q], -q});
         }
     }
-    return order;
 }
 
 // ---------------------------------------------------------------------------
@@ -244,167 +243,6 @@ __device__ __forceinline__ bool lp_wait(const unsigned* p, unsigned v, unsigned*
         __nanosleep(32);
     }
     return true;
-}
-
-// D(s): the diagonal tile by 8-row sub-panels in shared memory, as
-// k_ldl_diag does (ldlh.cu), with the 8 x 8 elimination spread over the
-// lanes of warp 0 (lane j owns column j of the sub-block; the pivot and the
-// rows of U reach the other lanes by shuffles).  Per pivot q the operations
-// and their order are those of the single-thread form: u_j = W(q, j) / d,
-// W(i, j) -= conj(u_i) W(q, j).
-template <bool CPLX>
-__device__ void lp_diag(cd* __restrict__ A, int ld, int n, int s, cd* __restrict__ dw, cd* __restrict__ invD,
-                        int* __restrict__ status, double2* sm)
-{
-    double2* Ws = sm;                   // Ws[r * LP_LD + c], r <= c
-    double2* Wu = sm + LDL_NB * LP_LD;  // Wu[q * 64 + c]: unscaled rows of the sub-panel
-    __shared__ double2 sid[LP_SUB];
-    const int p0 = s * LDL_NB, b = min(LDL_NB, n - p0);
-    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-    for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
-        const int r = e & 63, c = e >> 6;
-        double2 v = make_double2(0.0, 0.0);
-        if (r < b && c < b) {
-            if (r < c)
-                v = lp_ldcg(A + (size_t)(p0 + r) + (size_t)(p0 + c) * ld);
-            else if (r == c)
-                v = lp_ldcg(dw + p0 + r);
-        }
-        Ws[r * LP_LD + c] = v;
-    }
-    __syncthreads();
-    // 8 x 8 elimination of the sub-block at s0 by the 32 lanes of warp 0
-    auto eliminate = [&](int s0) {
-        const int nq = min(LP_SUB, b - s0);
-        const int j = lane;
-        const bool col = j < nq;
-        cd a[LP_SUB];
-#pragma unroll
-        for (int i = 0; i < LP_SUB; i++) {
-            double2 v = make_double2(0.0, 0.0);
-            if (col && i <= j) v = Ws[(s0 + i) * LP_LD + s0 + j];
-            a[i] = cd{v.x, v.y};
-        }
-#pragma unroll
-        for (int q = 0; q < LP_SUB; q++) {
-            if (q < nq) {
-                const cd dq = lp_shfl(a[q], q);  // W(q, q) from lane q
-                const double dr = dq.x, di = CPLX ? dq.y : 0.0;
-                const bool zero = (dr == 0.0 && di == 0.0);
-                double id, idi = 0.0;
-                if (CPLX) {
-                    const double m = zero ? 0.0 : __drcp_rn(fma(dr, dr, di * di));
-                    id = dr * m;
-                    idi = -di * m;
-                } else {
-                    id = zero ? 0.0 : __drcp_rn(dr);
-                }
-                if (lane == 0) {
-                    sid[q] = make_double2(id, idi);
-                    invD[p0 + s0 + q] = cd{id, idi};
-                    dw[p0 + s0 + q] = cd{dr, di};  // the pivot, for the trailing updates
-                    if (zero) atomicCAS(status + ST_ZERO_PIVOT, 0, p0 + s0 + q + 1);
-                }
-                cd u = cd{0.0, 0.0};
-                if (col && j > q) u = CPLX ? cmul(a[q], cd{id, idi}) : cd{a[q].x * id, a[q].y * id};  // U(q, j)
-#pragma unroll
-                for (int i = q + 1; i < LP_SUB; i++) {
-                    const cd ui = lp_shfl(u, i);
-                    if (col && j >= i) a[i] = cfms(conj(ui), a[q], a[i]);
-                }
-                if (col && j > q) a[q] = u;
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < LP_SUB; i++)
-            if (col && i < j) Ws[(s0 + i) * LP_LD + s0 + j] = make_double2(a[i].x, a[i].y);
-    };
-    if (wp == 0) eliminate(0);
-    __syncthreads();
-    for (int s0 = 0; s0 < b; s0 += LP_SUB) {
-        const int nq = min(LP_SUB, b - s0);
-        // (b) sub-panel rows beyond the sub-block, one thread per column
-        const int t0 = s0 + LP_SUB;
-        if (t0 < b && tid < b - t0) {
-            const int c = t0 + tid;
-            cd wun[LP_SUB];
-#pragma unroll
-            for (int q = 0; q < LP_SUB; q++) {
-                if (q < nq) {
-                    const double2 w = Ws[(s0 + q) * LP_LD + c];
-                    cd v = cd{w.x, w.y};
-#pragma unroll
-                    for (int q2 = 0; q2 < q; q2++) {
-                        const double2 u = Ws[(s0 + q2) * LP_LD + s0 + q];  // U(q2, q)
-                        v = cfms(cd{u.x, -u.y}, wun[q2], v);
-                    }
-                    wun[q] = v;
-                    Wu[q * LDL_NB + c] = make_double2(v.x, v.y);
-                    const double2 id = sid[q];
-                    const cd uq = CPLX ? cmul(v, cd{id.x, id.y}) : cd{v.x * id.x, v.y * id.x};
-                    Ws[(s0 + q) * LP_LD + c] = make_double2(uq.x, uq.y);
-                } else {
-                    wun[q] = cd{0.0, 0.0};
-                }
-            }
-        }
-        __syncthreads();
-        // (c) rank-8 update beyond the sub-panel on the FP64 tensor cores;
-        // warp 0 takes the next diagonal sub-block and eliminates it at once
-        if (t0 < b) {
-            const int g = lane >> 2, t4 = lane & 3;
-            const int T = (b - t0 + 7) >> 3;
-            const int ntiles = T * (T + 1) / 2;
-            for (int tile = (wp == 0) ? 0 : wp; tile < ntiles; tile += (wp == 0) ? ntiles : 7) {
-                int Rr = 0, rem = tile;
-                while (rem >= T - Rr) {
-                    rem -= T - Rr;
-                    Rr++;
-                }
-                const int Cc = Rr + rem;
-                const int r = t0 + 8 * Rr + g;
-                const int cg = t0 + 8 * Cc + g;
-                const int ca = t0 + 8 * Cc + 2 * t4;
-                double accr[2], acci[2];
-#pragma unroll
-                for (int e = 0; e < 2; e++) {
-                    const int c = ca + e;
-                    double2 w = make_double2(0.0, 0.0);
-                    if (r < b && c < b && r <= c) w = Ws[r * LP_LD + c];
-                    accr[e] = w.x;
-                    acci[e] = w.y;
-                }
-#pragma unroll
-                for (int k0 = 0; k0 < LP_SUB; k0 += 4) {
-                    const int q = k0 + t4;
-                    double2 u = make_double2(0.0, 0.0), v = make_double2(0.0, 0.0);
-                    if (q < nq && r < b) u = Ws[(s0 + q) * LP_LD + r];  // U(q, r)
-                    if (q < nq && cg < b) v = Wu[q * LDL_NB + cg];      // Wun(q, c)
-                    lp_mma(accr[0], accr[1], -u.x, v.x);
-                    lp_mma(accr[0], accr[1], -u.y, v.y);
-                    lp_mma(acci[0], acci[1], -u.x, v.y);
-                    lp_mma(acci[0], acci[1], u.y, v.x);
-                }
-#pragma unroll
-                for (int e = 0; e < 2; e++) {
-                    const int c = ca + e;
-                    if (r < b && c < b && r <= c) Ws[r * LP_LD + c] = make_double2(accr[e], acci[e]);
-                }
-            }
-            if (wp == 0) {
-                __syncwarp();
-                eliminate(t0);
-            }
-        }
-        __syncthreads();
-    }
-    for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
-        const int r = e & 63, c = e >> 6;
-        if (r < c && c < b) {
-            const double2 v = Ws[r * LP_LD + c];
-            A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld] = cd{v.x, v.y};
-        }
-    }
 }
 
 // T(s, C): U(s, C) = invD L_ss^-1 W(s, C) for the 64 columns of tile
@@ -472,7 +310,7 @@ __device__ void lp_trsm(cd* __restrict__ A, int ld, int n, int s, int C, const c
     __syncthreads();
     // the recurrence on this warp's eight columns
     const int c0 = 8 * wp;
-#pragma unroll
+#pragma unroll 1
     for (int bk = 0; bk < 8; bk++) {
         // Wun_b = X_b W_b
         double wr[2] = {0.0, 0.0}, wi[2] = {0.0, 0.0};
@@ -493,7 +331,7 @@ __device__ void lp_trsm(cd* __restrict__ A, int ld, int n, int s, int C, const c
         double2 un[2];
 #pragma unroll
         for (int k0 = 0; k0 < 8; k0 += 4) un[k0 / 4] = Wt[(8 * bk + k0 + t4) * LT_WP + c0 + g];  // Wun(k, c)
-#pragma unroll
+#pragma unroll 1
         for (int a = bk + 1; a < 8; a++) {
             double ar[2], ai[2];
 #pragma unroll
@@ -646,9 +484,6 @@ __device__ void lp_update(cd* __restrict__ A, int ld, int n, int s, int m, int R
             }
 }
 
-constexpr size_t lp_max(size_t a, size_t b) { return a > b ? a : b; }
-constexpr size_t LP_SMEM = lp_max(LP_SMEM_B, lp_max(LP_SMEM_D, LP_SMEM_T));
-
 struct LpArgs {
     cd* A;
     int ld, n, np;
@@ -668,6 +503,25 @@ __device__ __forceinline__ unsigned long long lp_clock()
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
+}
+
+// The tile counts a list task waits for: cnt[ix[i]] >= need[i], i < the
+// returned count.
+__device__ __forceinline__ int lp_deps(unsigned task, long long (&ix)[3], unsigned (&need)[3])
+{
+    const unsigned type = task >> 30;
+    const int s = (task >> 20) & 1023, R = (task >> 10) & 1023, C = task & 1023;
+    ix[1] = ix[2] = 0;
+    need[1] = need[2] = 0u;
+    if (type == LP_T) {
+        ix[0] = lp_tix(s, s), need[0] = (unsigned)s + 1;
+        ix[1] = lp_tix(s, C), need[1] = (unsigned)s;
+        return 2;
+    }
+    ix[0] = lp_tix(R, C), need[0] = (unsigned)s;
+    ix[1] = lp_tix(s, R), need[1] = (unsigned)s + 1;
+    ix[2] = lp_tix(s, C), need[2] = (unsigned)s + 1;
+    return (R == C) ? 2 : 3;
 }
 
 // Thread 0: wait until cnt[ix[i]] >= need[i] for the k (<= 3) conditions,
@@ -708,12 +562,9 @@ __device__ __forceinline__ void lp_trace(const LpArgs& a, unsigned code, int m, 
 
 // One task, all threads.  Thread 0 has checked the dependencies; on return
 // the task's stores are done (a barrier follows).  m: panels of an update.
-template <bool CPLX>
 __device__ __forceinline__ void lp_exec(const LpArgs& a, unsigned type, int s, int m, int R, int C, double2* sm)
 {
-    if (type == LP_D)
-        lp_diag<CPLX>(a.A, a.ld, a.n, s, a.dw, a.invD, a.status, sm);
-    else if (type == LP_T)
+    if (type == LP_T)
         lp_trsm(a.A, a.ld, a.n, s, C, a.invD, sm);
     else
         lp_update(a.A, a.ld, a.n, s, m, R, C, a.dw, sm);
@@ -724,6 +575,374 @@ __device__ __forceinline__ void lp_exec(const LpArgs& a, unsigned type, int s, i
 __device__ __forceinline__ void lp_publish(const LpArgs& a, long long ix, unsigned v)
 {
     if (threadIdx.x == 0) lp_st_release(a.cnt + ix, v);
+}
+
+// ---------------------------------------------------------------------------
+// The chain CTA.  It keeps the working diagonal tile (s, s) in shared
+// memory (its diagonal as dw holds it) and per panel s runs the three tasks
+// the next diagonal tile waits for:
+//   D(s)          elimination of the tile by 8-row sub-panels (8 x 8 blocks
+//                 by the lanes of warp 0, the rows beyond them by
+//                 substitution, rank-8 updates on the FP64 tensor cores,
+//                 the next block's elimination beside the update);
+//                 published at once, so the other panel rows start;
+//   T(s, s+1)     the tile to its right, by the blocked recurrence of
+//                 lp_trsm with L read from the tile in shared memory;
+//   B(s, s+1, s+1) tile (s+1, s+1) loaded once the other CTAs have applied
+//                 panels 0..s-1, then panel s applied from the panel rows
+//                 still in shared memory; it stays there for step s+1.
+// The tile (s+1, s+2) that T(s+1, s+2) needs comes from the other CTAs
+// (T(s, s+2), then B(s, s+1, s+2)) while this CTA runs D(s+1).
+constexpr int LC_NP = 2080;  // packed upper triangle of a 64 x 64 tile
+__device__ __forceinline__ int lc_pu(int r, int c) { return r * 64 - r * (r - 1) / 2 + (c - r); }  // r <= c
+constexpr size_t LP_SMEM_C = (size_t)(LC_NP + LDL_NB * LT_WP + 2 * LDL_NB + 8 * 64) * sizeof(double2);
+constexpr size_t lp_max(size_t a, size_t b) { return a > b ? a : b; }
+constexpr size_t LP_SMEM = lp_max(LP_SMEM_B, lp_max(LP_SMEM_C, LP_SMEM_T));
+
+template <bool CPLX>
+__device__ void lp_chain(const LpArgs& a, double2* sm, int limit)
+{
+    double2* P = sm;                      // packed tile: U_ss during T, tile (s+1, s+1) during B
+    double2* Rt = sm + LC_NP;             // right tile, Rt[q * LT_WP + c] (during T and B)
+    double2* Ws = Rt;                     // working diagonal tile, Ws[r * LP_LD + c] (during D)
+    double2* dpv = Rt + LDL_NB * LT_WP;   // pivots d of the panel
+    double2* sinv = dpv + LDL_NB;         // their inverses (invD)
+    double2* Xb = sinv + LDL_NB;          // X_b = L_bb^-1, Xb[b * 64 + i * 8 + j]
+    __shared__ double2 sid[LP_SUB];
+    __shared__ int s_go, s_v;
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int n = a.n, ld = a.ld;
+    cd* A = a.A;
+    // tile (0, 0) from global memory (upper triangle and dw)
+    for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
+        const int r = e & 63, c = e >> 6;
+        double2 v = make_double2(0.0, 0.0);
+        if (r <= c && c < min(LDL_NB, n)) v = (r < c) ? lp_ldcg(A + (size_t)r + (size_t)c * ld) : lp_ldcg(a.dw + r);
+        Ws[r * LP_LD + c] = v;
+    }
+    __syncthreads();
+    for (int s = 0; s < a.np; s++) {
+        const int p0 = s * LDL_NB, b = min(LDL_NB, n - p0);
+        const bool right = s + 1 < a.np;
+        const int cb = p0 + LDL_NB, wd = right ? min(LDL_NB, n - cb) : 0;
+        unsigned long long t0 = 0;
+        if (tid == 0 && a.trace) t0 = lp_clock();
+        // ================= D(s)
+        auto eliminate = [&](int s0) {  // warp 0: the 8 x 8 sub-block at s0
+            const int nq = min(LP_SUB, b - s0);
+            const int j = lane;
+            const bool col = j < nq;
+            cd x[LP_SUB];
+#pragma unroll
+            for (int i = 0; i < LP_SUB; i++) {
+                double2 v = make_double2(0.0, 0.0);
+                if (col && i <= j) v = Ws[(s0 + i) * LP_LD + s0 + j];
+                x[i] = cd{v.x, v.y};
+            }
+#pragma unroll
+            for (int q = 0; q < LP_SUB; q++) {
+                if (q < nq) {
+                    const cd dq = lp_shfl(x[q], q);
+                    const double dr = dq.x, di = CPLX ? dq.y : 0.0;
+                    const bool zero = (dr == 0.0 && di == 0.0);
+                    double id, idi = 0.0;
+                    if (CPLX) {
+                        const double m = zero ? 0.0 : __drcp_rn(fma(dr, dr, di * di));
+                        id = dr * m;
+                        idi = -di * m;
+                    } else {
+                        id = zero ? 0.0 : __drcp_rn(dr);
+                    }
+                    if (lane == 0) {
+                        sid[q] = make_double2(id, idi);
+                        dpv[s0 + q] = make_double2(dr, di);
+                        sinv[s0 + q] = make_double2(id, idi);
+                        a.invD[p0 + s0 + q] = cd{id, idi};
+                        a.dw[p0 + s0 + q] = cd{dr, di};
+                        if (zero) atomicCAS(a.status + ST_ZERO_PIVOT, 0, p0 + s0 + q + 1);
+                    }
+                    cd u = cd{0.0, 0.0};
+                    if (col && j > q) u = CPLX ? cmul(x[q], cd{id, idi}) : cd{x[q].x * id, x[q].y * id};
+#pragma unroll
+                    for (int i = q + 1; i < LP_SUB; i++) {
+                        const cd ui = lp_shfl(u, i);
+                        if (col && j >= i) x[i] = cfms(conj(ui), x[q], x[i]);
+                    }
+                    if (col && j > q) x[q] = u;
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < LP_SUB; i++)
+                if (col && i < j) Ws[(s0 + i) * LP_LD + s0 + j] = make_double2(x[i].x, x[i].y);
+        };
+        // s0 = -8: the first sub-block's elimination alone; then per
+        // sub-panel (b), (c) and the next elimination (one call site keeps
+        // the code small)
+        for (int s0 = -LP_SUB; s0 < b; s0 += LP_SUB) {
+            if (s0 < 0) {
+                if (wp == 0) eliminate(0);
+                __syncthreads();
+                continue;
+            }
+            const int nq = min(LP_SUB, b - s0);
+            const int t0c = s0 + LP_SUB;
+            if (t0c >= b) break;
+            // (b) sub-panel rows beyond the sub-block, one thread per column
+            if (tid < b - t0c) {
+                const int c = t0c + tid;
+                cd wun[LP_SUB];
+#pragma unroll
+                for (int q = 0; q < LP_SUB; q++) {
+                    if (q < nq) {
+                        double2* wq = Ws + (s0 + q) * LP_LD + c;
+                        const double2 w = *wq;
+                        cd v = cd{w.x, w.y};
+#pragma unroll
+                        for (int q2 = 0; q2 < q; q2++) {
+                            const double2 u = Ws[(s0 + q2) * LP_LD + s0 + q];  // U(q2, q)
+                            v = cfms(cd{u.x, -u.y}, wun[q2], v);
+                        }
+                        wun[q] = v;
+                        const double2 id = sid[q];
+                        const cd uq = CPLX ? cmul(v, cd{id.x, id.y}) : cd{v.x * id.x, v.y * id.x};
+                        *wq = make_double2(uq.x, uq.y);
+                    } else {
+                        wun[q] = cd{0.0, 0.0};
+                    }
+                }
+            }
+            __syncthreads();
+            // (c) rank-8 update of rows and columns [t0c, b), B operand
+            // d_q U(q, c); warp 0 takes the next diagonal sub-block and
+            // eliminates it at once
+            {
+                const int T = (b - t0c + 7) >> 3;
+                const int ntiles = T * (T + 1) / 2;
+                for (int tile = (wp == 0) ? 0 : wp; tile < ntiles; tile += (wp == 0) ? ntiles : 7) {
+                    int Rr = 0, rem = tile;
+                    while (rem >= T - Rr) {
+                        rem -= T - Rr;
+                        Rr++;
+                    }
+                    const int Cc = Rr + rem;
+                    const int r = t0c + 8 * Rr + g, cgc = t0c + 8 * Cc + g, ca = t0c + 8 * Cc + 2 * t4;
+                    double accr[2], acci[2];
+#pragma unroll
+                    for (int e = 0; e < 2; e++) {
+                        const int c = ca + e;
+                        double2 w = make_double2(0.0, 0.0);
+                        if (r < b && c < b && r <= c) w = Ws[(r) * LP_LD + c];
+                        accr[e] = w.x;
+                        acci[e] = w.y;
+                    }
+#pragma unroll
+                    for (int k0 = 0; k0 < LP_SUB; k0 += 4) {
+                        const int q = k0 + t4;
+                        double2 u = make_double2(0.0, 0.0), v = make_double2(0.0, 0.0);
+                        if (q < nq && r < b) u = Ws[(s0 + q) * LP_LD + r];  // U(q, r)
+                        if (q < nq && cgc < b) {
+                            const double2 uc = Ws[(s0 + q) * LP_LD + cgc];  // U(q, c)
+                            const double2 d = dpv[s0 + q];
+                            v = make_double2(fma(uc.x, d.x, -uc.y * d.y), fma(uc.x, d.y, uc.y * d.x));
+                        }
+                        lp_mma(accr[0], accr[1], -u.x, v.x);
+                        lp_mma(accr[0], accr[1], -u.y, v.y);
+                        lp_mma(acci[0], acci[1], -u.x, v.y);
+                        lp_mma(acci[0], acci[1], u.y, v.x);
+                    }
+#pragma unroll
+                    for (int e = 0; e < 2; e++) {
+                        const int c = ca + e;
+                        if (r < b && c < b && r <= c) Ws[(r) * LP_LD + c] = make_double2(accr[e], acci[e]);
+                    }
+                }
+                if (wp == 0) {
+                    __syncwarp();
+                    eliminate(t0c);
+                }
+            }
+            __syncthreads();
+        }
+        // U_ss out, and packed for T (the right tile overwrites Ws)
+        for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
+            const int r = e & 63, c = e >> 6;
+            if (r < c) {
+                const double2 v = Ws[r * LP_LD + c];
+                P[lc_pu(r, c)] = v;
+                if (c < b) A[(size_t)(p0 + r) + (size_t)(p0 + c) * ld] = cd{v.x, v.y};
+            }
+        }
+        __syncthreads();
+        lp_publish(a, lp_tix(s, s), (unsigned)s + 1);
+        if (tid == 0) lp_trace(a, lp_code(LP_D, s, s, s), 1, t0, t0);
+        if (!right) break;
+        // ================= T(s, s+1)
+        if (tid == 0) {
+            if (a.trace) t0 = lp_clock();
+            long long ix[3] = {lp_tix(s, s + 1), 0, 0};
+            unsigned need[3] = {(unsigned)s, 0u, 0u};
+            s_go = lp_wait_all(a, ix, need, 1, limit) ? 1 : 0;
+        }
+        __syncthreads();
+        if (!s_go) return;
+        unsigned long long t1 = 0;
+        if (tid == 0 && a.trace) t1 = lp_clock();
+        for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
+            const int q = e & 63, c = e >> 6;
+            const bool in = c < wd;
+            cp_async16(Rt + q * LT_WP + c, in ? (const void*)(A + (size_t)(p0 + q) + (size_t)(cb + c) * ld) : (const void*)A,
+                       in ? 16 : 0);
+        }
+        cp_async_commit();
+        {
+            // X_wp = L_bb^-1 of block bb = wp, L(r, q) = conj(U(q, r)); lane j < 8 holds column j
+            const int bb = wp, j = lane;
+            cd x[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) x[i] = cd{(i == j) ? 1.0 : 0.0, 0.0};
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+#pragma unroll
+                for (int r = q + 1; r < 8; r++) {
+                    const double2 u = P[lc_pu(8 * bb + q, 8 * bb + r)];
+                    x[r] = cfms(cd{u.x, -u.y}, x[q], x[r]);
+                }
+            if (j < 8)
+#pragma unroll
+                for (int i = 0; i < 8; i++) Xb[bb * 64 + i * 8 + j] = make_double2(x[i].x, x[i].y);
+        }
+        cp_async_wait<0>();
+        __syncthreads();
+        {
+            const int c0 = 8 * wp;
+#pragma unroll 1
+            for (int bk = 0; bk < 8; bk++) {
+                double wr[2] = {0.0, 0.0}, wi[2] = {0.0, 0.0};
+#pragma unroll
+                for (int k0 = 0; k0 < 8; k0 += 4) {
+                    const double2 xa = Xb[bk * 64 + g * 8 + k0 + t4];
+                    const double2 wv = Rt[(8 * bk + k0 + t4) * LT_WP + c0 + g];
+                    lp_mma(wr[0], wr[1], xa.x, wv.x);
+                    lp_mma(wr[0], wr[1], -xa.y, wv.y);
+                    lp_mma(wi[0], wi[1], xa.x, wv.y);
+                    lp_mma(wi[0], wi[1], xa.y, wv.x);
+                }
+                __syncwarp();
+#pragma unroll
+                for (int e = 0; e < 2; e++) Rt[(8 * bk + g) * LT_WP + c0 + 2 * t4 + e] = make_double2(wr[e], wi[e]);
+                __syncwarp();
+                double2 un[2];
+#pragma unroll
+                for (int k0 = 0; k0 < 8; k0 += 4) un[k0 / 4] = Rt[(8 * bk + k0 + t4) * LT_WP + c0 + g];
+#pragma unroll 1
+                for (int a2 = bk + 1; a2 < 8; a2++) {
+                    double ar[2], ai[2];
+#pragma unroll
+                    for (int e = 0; e < 2; e++) {
+                        const double2 o = Rt[(8 * a2 + g) * LT_WP + c0 + 2 * t4 + e];
+                        ar[e] = o.x;
+                        ai[e] = o.y;
+                    }
+#pragma unroll
+                    for (int k0 = 0; k0 < 8; k0 += 4) {
+                        const double2 uu = P[lc_pu(8 * bk + k0 + t4, 8 * a2 + g)];  // U(k, r): L(r, k) = conj
+                        const double2 u = un[k0 / 4];
+                        lp_mma(ar[0], ar[1], -uu.x, u.x);
+                        lp_mma(ar[0], ar[1], -uu.y, u.y);
+                        lp_mma(ai[0], ai[1], -uu.x, u.y);
+                        lp_mma(ai[0], ai[1], uu.y, u.x);
+                    }
+#pragma unroll
+                    for (int e = 0; e < 2; e++) Rt[(8 * a2 + g) * LT_WP + c0 + 2 * t4 + e] = make_double2(ar[e], ai[e]);
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // U(s, s+1) = invD Wun: kept in shared memory and written out
+        for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
+            const int q = e & 63, c = e >> 6;
+            const double2 v = Rt[q * LT_WP + c], d = sinv[q];
+            const cd u = cmul(cd{v.x, v.y}, cd{d.x, d.y});
+            Rt[q * LT_WP + c] = make_double2(u.x, u.y);
+            if (c < wd) A[(size_t)(p0 + q) + (size_t)(cb + c) * ld] = u;
+        }
+        __syncthreads();
+        lp_publish(a, lp_tix(s, s + 1), (unsigned)s + 1);
+        if (tid == 0) lp_trace(a, lp_code(LP_T, s, s, s + 1), 1, t0, t1);
+        // ================= B(s, s+1, s+1)
+        if (tid == 0) {
+            if (a.trace) t0 = lp_clock();
+            long long ix[3] = {lp_tix(s + 1, s + 1), 0, 0};
+            unsigned need[3] = {(unsigned)s, 0u, 0u};
+            const int go = lp_wait_all(a, ix, need, 1, limit) ? 1 : 0;
+            s_go = go;
+            s_v = go ? (int)lp_ld_acquire(a.cnt + ix[0]) : 0;
+            if (a.trace) t1 = lp_clock();
+        }
+        __syncthreads();
+        if (!s_go) return;
+        const int applied = s_v;  // panels already applied to tile (s+1, s+1)
+        const int q0 = p0 + LDL_NB, bn = min(LDL_NB, n - q0);
+        for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
+            const int r = e & 63, c = e >> 6;
+            if (r > c) continue;
+            double2 v = make_double2(0.0, 0.0);
+            if (c < bn) v = (r < c) ? lp_ldcg(A + (size_t)(q0 + r) + (size_t)(q0 + c) * ld) : lp_ldcg(a.dw + q0 + r);
+            P[lc_pu(r, c)] = v;
+        }
+        __syncthreads();
+        if (applied == s) {
+            // 8 x 8 tiles of the upper triangle; A = conj(U(q, r)), B = -(d_q U(q, c))
+            for (int tile = wp; tile < 36; tile += 8) {
+                int Rr = 0, rem = tile;
+                while (rem >= 8 - Rr) {
+                    rem -= 8 - Rr;
+                    Rr++;
+                }
+                const int Cc = Rr + rem;
+                const int r = 8 * Rr + g, cgc = 8 * Cc + g, ca = 8 * Cc + 2 * t4;
+                double accr[2], acci[2];
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int c = ca + e;
+                    double2 w = make_double2(0.0, 0.0);
+                    if (r <= c && c < bn) {
+                        w = P[lc_pu(r, c)];
+                        if (r == c) w.y = -w.y;  // dw keeps the conjugate of the upper-triangle value
+                    }
+                    accr[e] = w.x;
+                    acci[e] = w.y;
+                }
+#pragma unroll 2
+                for (int k0 = 0; k0 < LDL_NB; k0 += 4) {
+                    const int q = k0 + t4;
+                    const double2 u = Rt[q * LT_WP + r];
+                    const double2 uc = Rt[q * LT_WP + cgc];
+                    const double2 d = dpv[q];
+                    const double vr = -fma(uc.x, d.x, -uc.y * d.y), vi = -fma(uc.x, d.y, uc.y * d.x);
+                    lp_mma(accr[0], accr[1], u.x, vr);
+                    lp_mma(accr[0], accr[1], u.y, vi);
+                    lp_mma(acci[0], acci[1], u.x, vi);
+                    lp_mma(acci[0], acci[1], -u.y, vr);
+                }
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int c = ca + e;
+                    if (r <= c && c < bn) P[lc_pu(r, c)] = (r == c) ? make_double2(accr[e], -acci[e]) : make_double2(accr[e], acci[e]);
+                }
+            }
+        }
+        __syncthreads();
+        // the next diagonal tile into Ws (the right tile is no longer needed)
+        for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
+            const int r = e & 63, c = e >> 6;
+            Ws[r * LP_LD + c] = (r <= c) ? P[lc_pu(r, c)] : make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+        if (tid == 0) lp_trace(a, lp_code(LP_B, s, s + 1, s + 1), applied == s ? 1 : 0, t0, t1);
+    }
 }
 
 // CTA 0 runs the critical chain, per panel s: D(s), then T(s, s+1) and
@@ -768,35 +987,7 @@ __global__ void __launch_bounds__(256, 2) k_ldl_persist(LpArgs a)
     __syncthreads();
     if (!s_go) return;
     if (blockIdx.x == 0) {
-        for (int s = 0; s < a.np; s++) {
-            for (int step = 0; step < 3; step++) {
-                if (step > 0 && s + 1 >= a.np) break;
-                const unsigned type = (step == 0) ? LP_D : (step == 1) ? LP_T : LP_B;
-                const int R = (step == 2) ? s + 1 : s, C = (step == 0) ? s : s + 1;
-                const long long tix = lp_tix(R, C);
-                unsigned long long t0 = 0, t1 = 0;
-                if (tid == 0) {
-                    if (a.trace) t0 = lp_clock();
-                    long long ix[3] = {tix, 0, 0};
-                    unsigned need[3] = {(unsigned)s, 0u, 0u};
-                    int go = lp_wait_all(a, ix, need, 1, limit) ? 1 : 0;
-                    // an update already applied by a merged update is skipped
-                    if (go && step == 2 && lp_ld_acquire(a.cnt + tix) > (unsigned)s) go = 2;
-                    s_go = go;
-                    if (a.trace) t1 = lp_clock();
-                }
-                __syncthreads();
-                const int go = s_go;
-                if (!go) return;
-                if (go == 1) {
-                    lp_exec<CPLX>(a, type, s, 1, R, C, lsm);
-                    __syncthreads();
-                    lp_publish(a, tix, (unsigned)s + 1);
-                }
-                if (tid == 0) lp_trace(a, lp_code(type, s, R, C), go == 1 ? 1 : 0, t0, t1);
-                __syncthreads();  // s_go is rewritten by the next step
-            }
-        }
+        lp_chain<CPLX>(a, lsm, limit);
         return;
     }
     for (;;) {
@@ -816,18 +1007,7 @@ __global__ void __launch_bounds__(256, 2) k_ldl_persist(LpArgs a)
                 const int s = (task >> 20) & 1023, R = (task >> 10) & 1023, C = task & 1023;
                 long long ix[3] = {0, 0, 0};
                 unsigned need[3] = {0u, 0u, 0u};
-                int k = 0;
-                if (type == LP_D) {
-                    ix[0] = lp_tix(s, s), need[0] = (unsigned)s, k = 1;
-                } else if (type == LP_T) {
-                    ix[0] = lp_tix(s, s), need[0] = (unsigned)s + 1;
-                    ix[1] = lp_tix(s, C), need[1] = (unsigned)s, k = 2;
-                } else {
-                    ix[0] = lp_tix(R, C), need[0] = (unsigned)s;
-                    ix[1] = lp_tix(s, R), need[1] = (unsigned)s + 1;
-                    ix[2] = lp_tix(s, C), need[2] = (unsigned)s + 1;
-                    k = (R == C) ? 2 : 3;
-                }
+                const int k = lp_deps(task, ix, need);
                 go = lp_wait_all(a, ix, need, k, limit) ? 1 : 0;
                 if (go && type == LP_B) {
                     if (lp_ld_acquire(a.cnt + ix[0]) > (unsigned)s) {
@@ -844,7 +1024,13 @@ __global__ void __launch_bounds__(256, 2) k_ldl_persist(LpArgs a)
 #pragma unroll
                         for (int j = 1; j < LP_MERGE; j++) {
                             const unsigned want = (unsigned)(s + j) + 1;
-                            if (m == j && s + j < R && fr[j - 1] >= want && (R == C || fc[j - 1] >= want)) m = j + 1;
+                            // the lookahead panel of row R (s + j = R - 1) and, on a
+                            // diagonal tile, the one before it are left to their own
+                            // (short) tasks: a long merged update would hold up the
+                            // panel rows the chain waits for
+                            const bool own = (s + j == R - 1) || (R == C && s + j == R - 2);
+                            if (m == j && !own && s + j < R && fr[j - 1] >= want && (R == C || fc[j - 1] >= want))
+                                m = j + 1;
                         }
                     }
                 }
@@ -862,7 +1048,7 @@ __global__ void __launch_bounds__(256, 2) k_ldl_persist(LpArgs a)
         const unsigned type = task >> 30;
         const int s = (task >> 20) & 1023, R = (task >> 10) & 1023, C = task & 1023;
         if (go == 1) {
-            lp_exec<CPLX>(a, type, s, m, R, C, lsm);
+            lp_exec(a, type, s, m, R, C, lsm);
             __syncthreads();
             lp_publish(a, (type == LP_B) ? lp_tix(R, C) : lp_tix(s, (type == LP_D) ? s : C), (unsigned)(s + m));
         }
@@ -897,6 +1083,7 @@ int ldlp_grid(Ctx& c)
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c.dev);
     if (!coop || per_sm < 1) return 0;
     c.lp_grid = per_sm * sms;
+    c.lp_sms = sms;
     return c.lp_grid;
 }
 
@@ -909,7 +1096,9 @@ int ldlp_tasks(Ctx& c, int n, unsigned** tasks, int* count)
     if (grid <= 0) return -1;
     const int np = (n + LDL_NB - 1) / LDL_NB;
     if (np > 1023) return -1;
-    const std::vector<unsigned> list = lp_schedule(np, grid, LpCost());
+    const int per_sm = std::max(1, c.lp_grid / std::max(1, c.lp_sms));
+    std::vector<unsigned> list;
+    lp_schedule(np, std::max(1, grid - per_sm), LpCost(), list);
     unsigned* d = nullptr;
     if (cudaMalloc(&d, std::max<size_t>(1, list.size()) * sizeof(unsigned)) != cudaSuccess) {
         cudaGetLastError();
@@ -1000,8 +1189,8 @@ extern "C" int ecg_ldl_schedule(int n, int workers, unsigned* out, long long cap
     if (n < 1 || workers < 1 || !count) return -1;
     const int np = (n + LDL_NB - 1) / LDL_NB;
     if (np > 1023) return -1;
-    std::vector<unsigned> full;
-    lp_schedule(np, workers, LpCost(), &full);
+    std::vector<unsigned> full, list;
+    lp_schedule(np, workers, LpCost(), list, &full);
     *count = (long long)full.size();
     if (out && cap >= (long long)full.size()) std::copy(full.begin(), full.end(), out);
     return 0;
