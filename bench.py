@@ -368,8 +368,9 @@ def run_ours(args, dist):
         "pairs_hs": roof("fp64", hs_flop, st[0], peak_fma, "TFLOP/s",
                          "k_pair_energy<3> (+ k_pair_diag, k_prep): one launch per step", fma_src, "pairs_hs"),
         "ldlh": roof("tensor", ldl_flop, st[1], peak_tc, "TFLOP/s",
-                     "LDL^H factorisation, one CUDA-graph launch per step: k_ldl_bulk trailing updates on the "
-                     "FP64 tensor cores, k_ldl_diag / k_ldl_trsm panel kernels", tc_src, "ldlh"),
+                     "LDL^H factorisation, one CUDA-graph launch per step: the persistent tile kernel "
+                     "k_ldl_persist (trailing updates and panel rows on the FP64 tensor cores, the diagonal "
+                     "chain on its own CTA) between k_ldl_mirror and k_ldl_linv", tc_src, "ldlh"),
         "invit": roof("hbm", invit_bytes, st[2], peaks["hbm_gbs"], "GB/s",
                       "inverse iterations (k_hemv, k_fwd_coop, k_bwd_coop) + Rayleigh quotient", hbm_src, "invit"),
         "adjoint": roof("fp64", adj_flop, st[3], peak_fma, "TFLOP/s",
