@@ -19,6 +19,9 @@
 // src/linalg.f90:359-391 term for term; only the summation order differs,
 // and the pivots are kept real (the reference's complex arithmetic leaves a
 // rounding-level imaginary part in them).
+// A whole factorisation (m0 = 0) below LDL_PAIR_MIN rows runs instead as
+// the persistent tile kernel of ldlp.cu; ldlh_factor captures either form
+// into a CUDA graph.
 #include "ecg_internal.h"
 #include "zmma.cuh"
 
