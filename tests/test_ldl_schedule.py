@@ -68,6 +68,24 @@ def test_list_is_complete_and_topological(n, workers):
             assert pos[d] < pos[t], (t, d)
 
 
+def test_chain_tasks_in_chain_order():
+    """The chain CTA runs D(s), T(s, s+1), B(s, s+1, s+1) for s = 0, 1, ...
+    in that order: the start order must list them in that same order, so
+    that it stays a topological order of what each CTA actually runs (the
+    kernel's no-deadlock argument)."""
+    for n in (300, 4000):
+        lst = [decode(x) for x in schedule(n, 296)]
+        np_ = (n + NB - 1) // NB
+        chain = []
+        for s in range(np_):
+            chain.append((D_, s, s, s))
+            if s + 1 < np_:
+                chain += [(T_, s, s, s + 1), (B_, s, s + 1, s + 1)]
+        pos = {t: i for i, t in enumerate(lst)}
+        got = [pos[t] for t in chain]
+        assert got == sorted(got)
+
+
 def test_chain_tasks_lead_the_list():
     """The critical chain D(s) -> T(s, s+1) -> B(s, s+1, s+1) -> D(s+1)
     is taken early: every D(s+1) comes before the last update of panel s
