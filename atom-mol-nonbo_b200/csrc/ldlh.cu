@@ -785,9 +785,9 @@ int ldlh_factor_traced(Ctx& c, int n, unsigned long long* out, long long cap, lo
     }
     enqueue_persist(c, n, tasks, ntasks, d);
     unsigned recs = 0;
-    const size_t ntile = (size_t)nb * (nb + 1) / 2;  // trace records at ctl[2], ctl = counters + ntile
+    const size_t ntile = (size_t)nb * (nb + 1) / 2;  // trace records at ctl[2], ctl = counters + 2 ntile
     int r = 0;
-    if (cudaMemcpyAsync(&recs, c.lp_cnt + ntile + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, c.stream) !=
+    if (cudaMemcpyAsync(&recs, c.lp_cnt + 2 * ntile + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, c.stream) !=
             cudaSuccess ||
         cudaStreamSynchronize(c.stream) != cudaSuccess)
         r = -2;

@@ -54,9 +54,16 @@ constexpr int LP_SUB = 8;          // sub-panel rows of the diagonal elimination
 constexpr int LP_MERGE = 4;        // most panels one trailing update applies at once
 constexpr size_t LP_SMEM_B = (size_t)(LP_ST * LP_KC * 2 * LP_P + LP_MERGE * LDL_NB) * sizeof(double2);
 
-__host__ __device__ __forceinline__ unsigned lp_code(unsigned type, int s, int R, int C)
+__host__ __device__ __forceinline__ unsigned lp_code(unsigned type, int s, int R, int C, unsigned half = 0)
 {
-    return type << 30 | (unsigned)s << 20 | (unsigned)R << 10 | (unsigned)C;
+    return type << 30 | half << 29 | (unsigned)s << 20 | (unsigned)R << 10 | (unsigned)C;
+}
+// The updates of the two tile rows after panel s (the band the diagonal
+// chain waits on), except the chain's own B(s, s+1, s+1), run as two tasks
+// on the column halves of the tile, so each takes half the time on its SM.
+__host__ __device__ __forceinline__ bool lp_split(int s, int R, int C)
+{
+    return R <= s + 2 && !(R == s + 1 && C == s + 1);
 }
 // counter of tile (R, C), R <= C: column-wise packed triangle
 __host__ __device__ __forceinline__ long long lp_tix(int R, int C) { return (long long)C * (C + 1) / 2 + R; }
@@ -64,11 +71,13 @@ __host__ __device__ __forceinline__ long long lp_tix(int R, int C) { return (lon
 // ---------------------------------------------------------------------------
 // Host: the task list.
 // ---------------------------------------------------------------------------
-// Task durations (us) for the list scheduler, as measured on a B200 with
-// two CTAs per SM (globaltimer records of ecg_factor_trace); only their
-// ratios and the resulting priorities matter.
+// Task weights (us) for the list scheduler: the time a CTA is held by a
+// task on a B200 with two CTAs per SM, waits and merged updates included
+// (globaltimer records of ecg_factor_trace); a split update counts half.
+// Only the ratios matter: at K = 4000 this set measured 4.82 ms, the raw
+// run times (21, 24, 24, 15) 5.0 ms, and a T weighted above B 5.1-5.2 ms.
 struct LpCost {
-    double d = 21.0, t = 20.0, b = 24.0, bd = 15.0;
+    double d = 21.0, t = 40.0, b = 60.0, bd = 40.0;
 };
 
 // Tasks of a factorisation with np panels: the list the P CTAs other than
@@ -78,8 +87,10 @@ static void lp_schedule(int np, int P, const LpCost& cost, std::vector<unsigned>
                         std::vector<unsigned>* full = nullptr)
 {
     std::vector<unsigned> code;
-    std::vector<long long> idD(np), baseB(np);
+    std::vector<long long> idD(np);
     std::vector<long long> idT((size_t)np * np, -1);
+    std::vector<long long> idB((size_t)np * np * np, -1);  // first node of B(s, R, C)
+    auto bix = [&](int s, int R, int C) -> size_t { return ((size_t)s * np + R) * np + C; };
     for (int s = 0; s < np; s++) {
         idD[s] = (long long)code.size();
         code.push_back(lp_code(LP_D, s, s, s));
@@ -87,48 +98,55 @@ static void lp_schedule(int np, int P, const LpCost& cost, std::vector<unsigned>
             idT[(size_t)s * np + C] = (long long)code.size();
             code.push_back(lp_code(LP_T, s, s, C));
         }
-        baseB[s] = (long long)code.size();
         for (int R = s + 1; R < np; R++)
-            for (int C = R; C < np; C++) code.push_back(lp_code(LP_B, s, R, C));
+            for (int C = R; C < np; C++) {
+                idB[bix(s, R, C)] = (long long)code.size();
+                code.push_back(lp_code(LP_B, s, R, C));
+                if (lp_split(s, R, C)) code.push_back(lp_code(LP_B, s, R, C, 1));  // the second column half
+            }
     }
-    auto idB = [&](int s, int R, int C) -> long long {
-        const long long off = (long long)(R - s - 1) * np - ((long long)(R - 1) * R / 2 - (long long)s * (s + 1) / 2);
-        return baseB[s] + off + (C - R);
-    };
     const long long N = (long long)code.size();
-    // predecessors (at most three) in creation order, which is topological
-    std::vector<long long> pred((size_t)N * 3, -1);
+    // predecessors in creation order, which is topological: an update that
+    // is split in two column halves counts as both halves
+    constexpr int NPRED = 6;
+    std::vector<long long> pred((size_t)N * NPRED, -1);
     std::vector<double> w((size_t)N);
     for (long long t = 0; t < N; t++) {
         const unsigned c = code[t];
-        const int type = c >> 30, s = (c >> 20) & 1023, R = (c >> 10) & 1023, C = c & 1023;
-        long long* p = &pred[(size_t)t * 3];
+        const int type = c >> 30, s = (c >> 20) & 511, R = (c >> 10) & 1023, C = c & 1023;
+        long long* p = &pred[(size_t)t * NPRED];
+        int k = 0;
+        auto addB = [&](int s2, int R2, int C2) {
+            const long long b = idB[bix(s2, R2, C2)];
+            p[k++] = b;
+            if (lp_split(s2, R2, C2)) p[k++] = b + 1;
+        };
         if (type == LP_D) {
-            if (s > 0) p[0] = idB(s - 1, s, s);
+            if (s > 0) addB(s - 1, s, s);
             w[t] = cost.d;
         } else if (type == LP_T) {
-            p[0] = idD[s];
-            if (s > 0) p[1] = idB(s - 1, s, C);
+            p[k++] = idD[s];
+            if (s > 0) addB(s - 1, s, C);
             w[t] = cost.t;
         } else {
-            p[0] = idT[(size_t)s * np + R];
-            if (C != R) p[1] = idT[(size_t)s * np + C];
-            if (s > 0) p[2] = idB(s - 1, R, C);
-            w[t] = (R == C) ? cost.bd : cost.b;
+            p[k++] = idT[(size_t)s * np + R];
+            if (C != R) p[k++] = idT[(size_t)s * np + C];
+            if (s > 0) addB(s - 1, R, C);
+            w[t] = ((R == C) ? cost.bd : cost.b) * (lp_split(s, R, C) ? 0.5 : 1.0);
         }
     }
     // successors (CSR)
     std::vector<long long> so((size_t)N + 1, 0), sl;
     for (long long t = 0; t < N; t++)
-        for (int k = 0; k < 3; k++)
-            if (pred[(size_t)t * 3 + k] >= 0) so[(size_t)pred[(size_t)t * 3 + k] + 1]++;
+        for (int k = 0; k < NPRED; k++)
+            if (pred[(size_t)t * NPRED + k] >= 0) so[(size_t)pred[(size_t)t * NPRED + k] + 1]++;
     for (long long t = 0; t < N; t++) so[(size_t)t + 1] += so[(size_t)t];
     sl.resize((size_t)so[(size_t)N]);
     {
         std::vector<long long> fill(so.begin(), so.end() - 1);
         for (long long t = 0; t < N; t++)
-            for (int k = 0; k < 3; k++) {
-                const long long p = pred[(size_t)t * 3 + k];
+            for (int k = 0; k < NPRED; k++) {
+                const long long p = pred[(size_t)t * NPRED + k];
                 if (p >= 0) sl[(size_t)fill[(size_t)p]++] = t;
             }
     }
@@ -150,7 +168,7 @@ static void lp_schedule(int np, int P, const LpCost& cost, std::vector<unsigned>
         pool[(size_t)idD[s]] = 0;
         cseq.push_back(idD[s]);
         if (s + 1 < np) {
-            const long long t = idT[(size_t)s * np + s + 1], b = idB(s, s + 1, s + 1);
+            const long long t = idT[(size_t)s * np + s + 1], b = idB[bix(s, s + 1, s + 1)];
             pool[(size_t)t] = pool[(size_t)b] = 0;
             cseq.push_back(t);
             cseq.push_back(b);
@@ -158,7 +176,7 @@ static void lp_schedule(int np, int P, const LpCost& cost, std::vector<unsigned>
     }
     std::vector<int> npred((size_t)N, 0);
     for (long long t = 0; t < N; t++)
-        for (int k = 0; k < 3; k++) npred[(size_t)t] += pred[(size_t)t * 3 + k] >= 0;
+        for (int k = 0; k < NPRED; k++) npred[(size_t)t] += pred[(size_t)t * NPRED + k] >= 0;
     typedef std::pair<double, long long> Item;
     std::priority_queue<Item> ready;                                        // (rank, -id)
     std::priority_queue<Item, std::vector<Item>, std::greater<Item>> busy;  // (finish, id)
@@ -373,20 +391,24 @@ __device__ void lp_trsm(cd* __restrict__ A, int ld, int n, int s, int C, const c
 // rows.  m consecutive panels s..s+m-1 (whose rows are contiguous) are
 // applied in one pass when they are all ready: a rank-64m update, the
 // tile read and written once.
-__device__ void lp_update(cd* __restrict__ A, int ld, int n, int s, int m, int R, int C, cd* __restrict__ dw,
-                          double2* sm)
+// MT x NT mma tiles per warp, WR x WC warps: <4, 2, 2, 4> covers the whole
+// 64 x 64 tile, <2, 2, 4, 2> the 64 x 32 column half `half` of it.
+template <int MT, int NT, int WR, int WC>
+__device__ void lp_update(cd* __restrict__ A, int ld, int n, int s, int m, int R, int C, int half,
+                          cd* __restrict__ dw, double2* sm)
 {
-    constexpr int MT = 4, NT = 2;
+    static_assert(WR * WC == 8 && WR * MT * 8 == LDL_NB, "eight warps over the 64 tile rows");
+    constexpr int CW = WC * NT * 8;  // columns covered
     const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-    const int wr = wp >> 2, wc = wp & 3;
+    const int wr = wp / WC, wc = wp % WC;
     const int g = lane >> 2, t4 = lane & 3;
     const int p0 = s * LDL_NB, b = min(m * LDL_NB, n - p0);
-    const int rb = R * LDL_NB, cb = C * LDL_NB;
+    const int rb = R * LDL_NB, cb = C * LDL_NB + half * CW;
     const bool dtile = (R == C);
     double2* dp = sm + LP_ST * LP_KC * 2 * LP_P;  // pivots d_q of panels s..s+m-1
     for (int q = tid; q < m * LDL_NB; q += 256) dp[q] = q < b ? lp_ldcg(dw + p0 + q) : make_double2(0.0, 0.0);
     // a warp whose sub-tile lies wholly below the diagonal has nothing to do
-    const bool wact = !dtile || (wr * 32 <= wc * 16 + 15);
+    const bool wact = !dtile || (wr * MT * 8 <= half * CW + (wc + 1) * NT * 8 - 1);
     auto stage = [&](int ch, int buf) {
         const int k0 = ch * LP_KC;
         double2* Us = sm + buf * LP_KC * 2 * LP_P;
@@ -395,10 +417,16 @@ __device__ void lp_update(cd* __restrict__ A, int ld, int n, int s, int m, int R
         for (int e = tid; e < LP_KC * LDL_NB; e += 256) {
             const int q = e % LP_KC, mm = e / LP_KC;
             const bool kq = k0 + q < b;
-            const int r = rb + mm, c = cb + mm;
-            const bool ku = kq && r < n, kv = kq && c < n;
+            const int r = rb + mm;
+            const bool ku = kq && r < n;
             cp_async16(Us + q * LP_P + mm, ku ? (const void*)(A + (size_t)(p0 + k0 + q) + (size_t)r * ld) : (const void*)A,
                        ku ? 16 : 0);
+        }
+#pragma unroll
+        for (int e = tid; e < LP_KC * CW; e += 256) {
+            const int q = e % LP_KC, mm = e / LP_KC;
+            const int c = cb + mm;
+            const bool kv = (k0 + q < b) && c < n;
             cp_async16(Vs + q * LP_P + mm, kv ? (const void*)(A + (size_t)(p0 + k0 + q) + (size_t)c * ld) : (const void*)A,
                        kv ? 16 : 0);
         }
@@ -490,6 +518,7 @@ struct LpArgs {
     const unsigned* tasks;  // the list of the CTAs other than the chain CTA
     int ntasks;
     unsigned* cnt;          // tile counters
+    unsigned* hc;           // per tile: column halves of band updates finished
     unsigned* ctl;          // [0] next list index, [1] abort word, [2] trace records, [3] chain CTA's SM + 1
     cd* dw;
     cd* invD;
@@ -510,7 +539,7 @@ __device__ __forceinline__ unsigned long long lp_clock()
 __device__ __forceinline__ int lp_deps(unsigned task, long long (&ix)[3], unsigned (&need)[3])
 {
     const unsigned type = task >> 30;
-    const int s = (task >> 20) & 1023, R = (task >> 10) & 1023, C = task & 1023;
+    const int s = (task >> 20) & 511, R = (task >> 10) & 1023, C = task & 1023;
     ix[1] = ix[2] = 0;
     need[1] = need[2] = 0u;
     if (type == LP_T) {
@@ -562,12 +591,15 @@ __device__ __forceinline__ void lp_trace(const LpArgs& a, unsigned code, int m, 
 
 // One task, all threads.  Thread 0 has checked the dependencies; on return
 // the task's stores are done (a barrier follows).  m: panels of an update.
-__device__ __forceinline__ void lp_exec(const LpArgs& a, unsigned type, int s, int m, int R, int C, double2* sm)
+__device__ __forceinline__ void lp_exec(const LpArgs& a, unsigned type, int s, int m, int R, int C, int half,
+                                        double2* sm)
 {
     if (type == LP_T)
         lp_trsm(a.A, a.ld, a.n, s, C, a.invD, sm);
+    else if (lp_split(s, R, C))
+        lp_update<2, 2, 4, 2>(a.A, a.ld, a.n, s, 1, R, C, half, a.dw, sm);
     else
-        lp_update(a.A, a.ld, a.n, s, m, R, C, a.dw, sm);
+        lp_update<4, 2, 2, 4>(a.A, a.ld, a.n, s, m, R, C, 0, a.dw, sm);
 }
 
 // After the task's barrier: thread 0 publishes the tile's new count.  The
@@ -1004,7 +1036,7 @@ __global__ void __launch_bounds__(256, 2) k_ldl_persist(LpArgs a)
             int go = 0, m = 1;
             if (task != LP_NONE) {
                 const unsigned type = task >> 30;
-                const int s = (task >> 20) & 1023, R = (task >> 10) & 1023, C = task & 1023;
+                const int s = (task >> 20) & 511, R = (task >> 10) & 1023, C = task & 1023;
                 long long ix[3] = {0, 0, 0};
                 unsigned need[3] = {0u, 0u, 0u};
                 const int k = lp_deps(task, ix, need);
@@ -1012,7 +1044,7 @@ __global__ void __launch_bounds__(256, 2) k_ldl_persist(LpArgs a)
                 if (go && type == LP_B) {
                     if (lp_ld_acquire(a.cnt + ix[0]) > (unsigned)s) {
                         go = 2;  // applied already by a merged update
-                    } else {
+                    } else if (!lp_split(s, R, C)) {
                         // following panels whose rows of R and C are final
                         unsigned fr[LP_MERGE - 1], fc[LP_MERGE - 1];
 #pragma unroll
@@ -1024,11 +1056,11 @@ __global__ void __launch_bounds__(256, 2) k_ldl_persist(LpArgs a)
 #pragma unroll
                         for (int j = 1; j < LP_MERGE; j++) {
                             const unsigned want = (unsigned)(s + j) + 1;
-                            // the lookahead panel of row R (s + j = R - 1) and, on a
-                            // diagonal tile, the one before it are left to their own
-                            // (short) tasks: a long merged update would hold up the
-                            // panel rows the chain waits for
-                            const bool own = (s + j == R - 1) || (R == C && s + j == R - 2);
+                            // the panels of the band next to row R (split in column
+                            // halves) and the chain's own update keep their own short
+                            // tasks: a long merged update would hold up the panel rows
+                            // the chain waits for
+                            const bool own = lp_split(s + j, R, C) || (s + j == R - 1);
                             if (m == j && !own && s + j < R && fr[j - 1] >= want && (R == C || fc[j - 1] >= want))
                                 m = j + 1;
                         }
@@ -1046,11 +1078,22 @@ __global__ void __launch_bounds__(256, 2) k_ldl_persist(LpArgs a)
         const int go = s_go, m = s_m;
         if (task == LP_NONE) return;
         const unsigned type = task >> 30;
-        const int s = (task >> 20) & 1023, R = (task >> 10) & 1023, C = task & 1023;
+        const int s = (task >> 20) & 511, R = (task >> 10) & 1023, C = task & 1023;
+        const int half = (task >> 29) & 1;
         if (go == 1) {
-            lp_exec(a, type, s, m, R, C, lsm);
+            lp_exec(a, type, s, m, R, C, half, lsm);
             __syncthreads();
-            lp_publish(a, (type == LP_B) ? lp_tix(R, C) : lp_tix(s, (type == LP_D) ? s : C), (unsigned)(s + m));
+            const long long tt = (type == LP_B) ? lp_tix(R, C) : lp_tix(s, (type == LP_D) ? s : C);
+            if (type == LP_B && lp_split(s, R, C)) {
+                // a column half: the second of the two to finish publishes the tile
+                if (tid == 0) {
+                    unsigned old;
+                    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(a.hc + tt) : "memory");
+                    if (old & 1u) lp_st_release(a.cnt + tt, (unsigned)s + 1);
+                }
+            } else {
+                lp_publish(a, tt, (unsigned)(s + m));
+            }
         }
         if (tid == 0) lp_trace(a, task, go == 1 ? m : 0, t0, t1);
         __syncthreads();  // s_next, s_go, s_m are rewritten by the next task
@@ -1095,7 +1138,7 @@ int ldlp_tasks(Ctx& c, int n, unsigned** tasks, int* count)
     const int grid = ldlp_grid(c);
     if (grid <= 0) return -1;
     const int np = (n + LDL_NB - 1) / LDL_NB;
-    if (np > 1023) return -1;
+    if (np > 200) return -1;
     const int per_sm = std::max(1, c.lp_grid / std::max(1, c.lp_sms));
     std::vector<unsigned> list;
     lp_schedule(np, std::max(1, grid - per_sm), LpCost(), list);
@@ -1118,14 +1161,16 @@ int ldlp_tasks(Ctx& c, int n, unsigned** tasks, int* count)
 long long ldlp_task_total(int n)
 {
     const long long np = (n + LDL_NB - 1) / LDL_NB;
-    return np + np * (np - 1) / 2 + (np - 1) * np * (np + 1) / 6;
+    long long split = 0;  // the second column halves of the band updates
+    for (long long s = 0; s + 2 < np; s++) split += 2 * (np - s - 2);
+    return np + np * (np - 1) / 2 + (np - 1) * np * (np + 1) / 6 + split;
 }
 
 // Tile counters and the control words (next task, abort word, trace
 // records, the chain CTA's SM) for np panels.
 int ldlp_reserve(Ctx& c, int np)
 {
-    const size_t need = (size_t)np * (np + 1) / 2 + 4;
+    const size_t need = (size_t)np * (np + 1) + 4;
     if (c.lp_cap >= need) return 0;
     if (c.lp_cnt) cudaFree(c.lp_cnt);
     c.lp_cnt = nullptr;
@@ -1145,7 +1190,7 @@ void ldlp_enqueue(Ctx& c, int n, const unsigned* tasks, int ntasks, unsigned lon
 {
     const int np = (n + LDL_NB - 1) / LDL_NB;
     const size_t ntile = (size_t)np * (np + 1) / 2;
-    cudaMemsetAsync(c.lp_cnt, 0, (ntile + 4) * sizeof(unsigned), c.stream);
+    cudaMemsetAsync(c.lp_cnt, 0, (2 * ntile + 4) * sizeof(unsigned), c.stream);
     LpArgs a;
     a.A = c.F;
     a.ld = c.ld;
@@ -1154,7 +1199,8 @@ void ldlp_enqueue(Ctx& c, int n, const unsigned* tasks, int ntasks, unsigned lon
     a.tasks = tasks;
     a.ntasks = ntasks;
     a.cnt = c.lp_cnt;
-    a.ctl = c.lp_cnt + ntile;
+    a.hc = c.lp_cnt + ntile;
+    a.ctl = c.lp_cnt + 2 * ntile;
     a.dw = c.dw;
     a.invD = c.invD;
     a.status = c.status;
@@ -1188,7 +1234,7 @@ extern "C" int ecg_ldl_schedule(int n, int workers, unsigned* out, long long cap
     using namespace ecg;
     if (n < 1 || workers < 1 || !count) return -1;
     const int np = (n + LDL_NB - 1) / LDL_NB;
-    if (np > 1023) return -1;
+    if (np > 200) return -1;
     std::vector<unsigned> full, list;
     lp_schedule(np, workers, LpCost(), list, &full);
     *count = (long long)full.size();

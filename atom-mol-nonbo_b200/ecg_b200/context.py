@@ -418,6 +418,7 @@ class Context:
         cnt = C.c_longlong()
         np_ = (n + 63) // 64
         total = np_ + np_ * (np_ - 1) // 2 + (np_ - 1) * np_ * (np_ + 1) // 6
+        total += sum(2 * (np_ - s - 2) for s in range(max(0, np_ - 2)))  # band updates in two halves
         out = np.zeros((total, 4), dtype=np.uint64)
         _check(self.lib.ecg_factor_trace(self.h, int(n), C.c_void_p(out.ctypes.data), out.size, C.byref(cnt)),
                "ecg_factor_trace")

@@ -347,13 +347,14 @@ int ecg_factor_trace(ecg_ctx* ctx, int n, unsigned long long* records, long long
  * No counterpart in the reference: a diagnostic that lets a test make a
  * wait run out without a fault. */
 int ecg_set_wait_limit(ecg_ctx* ctx, int polls);
-/* The task list of the persistent factorisation of n rows for `workers`
- * CTAs, on the host (no GPU needed): codes type << 30 | s << 20 | R << 10 |
- * C, type 0 = D(s) (diagonal tile s), 1 = T(s, C) (panel rows of tile
- * (s, C)), 2 = B(s, R, C) (update of tile (R, C) by panel s), 64-row
- * tiles.  *count receives the length; out (capacity cap) is filled when it
- * is large enough.  No counterpart in the reference: exposes the task order
- * to tests. */
+/* The task order of the persistent factorisation of n rows (n <= 12800)
+ * for a grid of `workers` CTAs, on the host (no GPU needed): codes
+ * type << 30 | h << 29 | s << 20 | R << 10 | C, type 0 = D(s) (diagonal
+ * tile s), 1 = T(s, C) (panel rows of tile (s, C)), 2 = B(s, R, C) (update
+ * of tile (R, C) by panel s; for R <= s + 2, other than (s+1, s+1), two
+ * tasks on the column halves h = 0, 1), 64-row tiles.  *count receives the
+ * length; out (capacity cap) is filled when it is large enough.  No
+ * counterpart in the reference: exposes the task order to tests. */
 int ecg_ldl_schedule(int n, int workers, unsigned* out, long long cap, long long* count);
 /* Bytes this context has copied host->device and device->host so far. */
 int ecg_io_bytes(ecg_ctx* ctx, long long* h2d, long long* d2h);

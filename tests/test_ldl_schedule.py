@@ -27,33 +27,46 @@ def schedule(n, workers):
 
 
 def decode(code):
+    """(type, s, R, C, column half)."""
     code = int(code)
-    return code >> 30, (code >> 20) & 1023, (code >> 10) & 1023, code & 1023
+    return code >> 30, (code >> 20) & 511, (code >> 10) & 1023, code & 1023, (code >> 29) & 1
+
+
+def split(s, r, c):
+    """The updates of the two tile rows after panel s, except the chain's
+    B(s, s+1, s+1), run as two column halves."""
+    return r <= s + 2 and not (r == s + 1 and c == s + 1)
 
 
 def expected_tasks(np_):
     t = set()
     for s in range(np_):
-        t.add((D_, s, s, s))
+        t.add((D_, s, s, s, 0))
         for c in range(s + 1, np_):
-            t.add((T_, s, s, c))
+            t.add((T_, s, s, c, 0))
         for r in range(s + 1, np_):
             for c in range(r, np_):
-                t.add((B_, s, r, c))
+                t.add((B_, s, r, c, 0))
+                if split(s, r, c):
+                    t.add((B_, s, r, c, 1))
     return t
 
 
+def upd(s, r, c):
+    return [(B_, s, r, c, h) for h in ((0, 1) if split(s, r, c) else (0,))]
+
+
 def deps(task):
-    ty, s, r, c = task
+    ty, s, r, c, _ = task
     if ty == D_:
-        return [(B_, s - 1, s, s)] if s > 0 else []
+        return upd(s - 1, s, s) if s > 0 else []
     if ty == T_:
-        return [(D_, s, s, s)] + ([(B_, s - 1, s, c)] if s > 0 else [])
-    d = [(T_, s, s, r)]
+        return [(D_, s, s, s, 0)] + (upd(s - 1, s, c) if s > 0 else [])
+    d = [(T_, s, s, r, 0)]
     if c != r:
-        d.append((T_, s, s, c))
+        d.append((T_, s, s, c, 0))
     if s > 0:
-        d.append((B_, s - 1, r, c))
+        d += upd(s - 1, r, c)
     return d
 
 
@@ -78,9 +91,9 @@ def test_chain_tasks_in_chain_order():
         np_ = (n + NB - 1) // NB
         chain = []
         for s in range(np_):
-            chain.append((D_, s, s, s))
+            chain.append((D_, s, s, s, 0))
             if s + 1 < np_:
-                chain += [(T_, s, s, s + 1), (B_, s, s + 1, s + 1)]
+                chain += [(T_, s, s, s + 1, 0), (B_, s, s + 1, s + 1, 0)]
         pos = {t: i for i, t in enumerate(lst)}
         got = [pos[t] for t in chain]
         assert got == sorted(got)
@@ -94,8 +107,8 @@ def test_chain_tasks_lead_the_list():
     pos = {t: i for i, t in enumerate(lst)}
     np_ = (4000 + NB - 1) // NB
     for s in range(np_ - 4):
-        last_b = max(pos[(B_, s, r, c)] for r in range(s + 1, np_) for c in range(r, np_))
-        assert pos[(D_, s + 1, s + 1, s + 1)] < last_b
+        last_b = max(pos[(B_, s, r, c, 0)] for r in range(s + 1, np_) for c in range(r, np_))
+        assert pos[(D_, s + 1, s + 1, s + 1, 0)] < last_b
 
 
 def run_tasks(M, lst, complex_pivots=False):
@@ -104,7 +117,7 @@ def run_tasks(M, lst, complex_pivots=False):
     W = np.triu(M.conj().T).copy()   # working upper triangle W(r, c) = M(c, r)^*
     U = np.zeros_like(W)
     d = np.zeros(n, dtype=complex)
-    for ty, s, r, c in lst:
+    for ty, s, r, c, h in lst:
         p0, p1 = s * NB, min(n, s * NB + NB)
         if ty == D_:
             Wb = W[p0:p1, p0:p1].copy()
@@ -124,9 +137,13 @@ def run_tasks(M, lst, complex_pivots=False):
         else:
             r0, r1 = r * NB, min(n, r * NB + NB)
             c0, c1 = c * NB, min(n, c * NB + NB)
+            if split(s, r, c):  # one column half of the tile
+                c0, c1 = c0 + 32 * h, min(c1, c0 + 32 * h + 32)
+            if c1 <= c0:
+                continue
             upd = U[p0:p1, r0:r1].conj().T @ (d[p0:p1, None] * U[p0:p1, c0:c1])
             if r == c:
-                upd = np.triu(upd)
+                upd = np.triu(upd, r0 - c0)  # keep global column >= global row
             W[r0:r1, c0:c1] -= upd
     return U, d
 
