@@ -64,7 +64,7 @@ void free_ctx(Ctx& c)
     if (c.F && c.F != c.H) cudaFree(c.F);
     if (c.gcnt_h) cudaFreeHost(c.gcnt_h);
     void* ptrs[] = {c.gcnt, c.params, c.H, c.S, c.diagS, c.diagH, c.invD, c.c, c.x, c.w, c.D, c.grad, c.Pd, c.coef,
-                    c.bra, c.ket, c.detL, c.part, c.dw, c.linv, c.vbuf, c.status, c.red, c.counters, c.yv,
+                    c.bra, c.ket, c.detL, c.part, c.dw, c.linv, c.lmf, c.lnb, c.vbuf, c.status, c.red, c.counters, c.yv,
                     c.zv, c.spart, c.colval, c.dblk, c.flags};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -517,6 +517,8 @@ int ecg_ctx_create(int n, const double* mass_matrix_host, const double* charges_
     r |= dalloc(&c.detL, L);
     r |= dalloc(&c.dw, L);
     r |= dalloc(&c.linv, L * LDL_NB);
+    r |= dalloc(&c.lmf, L * LDL_NB);
+    r |= dalloc(&c.lnb, L * LDL_NB);
     r |= dalloc(&c.vbuf, 3 * L * LDL_VLD);
     r |= dalloc(&c.status, (size_t)ST_COUNT);
     r |= dalloc(&c.red, (size_t)RD_COUNT);

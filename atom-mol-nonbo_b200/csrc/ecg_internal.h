@@ -141,6 +141,8 @@ struct Ctx {
     // LDL^H workspace
     cd* dw = nullptr;           // working diagonal (ld)
     cd* linv = nullptr;         // ld x LDL_NB: inverse unit-lower diagonal blocks
+    cd* lmf = nullptr;          // ld x LDL_NB: Linv_j U(j-1, j)^H per panel (forward solves)
+    cd* lnb = nullptr;          // ld x LDL_NB: Linv_j^H U(j, j+1) per panel (backward solves)
     cd* vbuf = nullptr;         // 3 x LDL_VLD x ld: unscaled rows of a panel (pair) (rotating)
     int* status = nullptr;      // device status words (see ST_*)
     int* status_h = nullptr;    // pinned host mirror
@@ -159,6 +161,7 @@ struct Ctx {
     unsigned* flags = nullptr;  // per-panel ready flags of the cooperative solves (ld + 2)
     unsigned epoch = 0;         // value a panel flag takes when its panel is solved
     int coop_max_blocks = 0;    // co-resident CTAs of the cooperative solve kernels
+    int coop_max_neigh = 0;     // the same with the neighbour products in shared memory
     std::vector<int> blk_start; // block starts of the current LDL^H factor
     // captured LDL^H factorisations, keyed by (m0, n, existing block starts)
     struct LdlGraph {

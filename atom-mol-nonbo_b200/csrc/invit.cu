@@ -152,7 +152,12 @@ __global__ void __launch_bounds__(256) k_bwd(const cd* __restrict__ A, int ld, i
 // co-resident (cooperative launch).  CTA j accumulates the contributions of
 // the panels it depends on in panel order, each as soon as that panel's
 // flag carries the current epoch (acquire / release), then applies its
-// inverse diagonal block and publishes its own panel.  Every wait is
+// inverse diagonal block and publishes its own panel.  The neighbouring
+// panel (j-1 forward, j+1 backward) is left out of that sum: its term is
+// applied after the inverse block as one 64 x 64 product with the
+// precomputed M_j = Linv_j U(j-1, j)^H or N_j = Linv_j^H U(j, j+1)
+// (k_ldl_mn), so the step from one panel's flag to the next is that
+// product alone.  Every wait is
 // bounded: after SOLVE_SPIN_LIMIT polls, or as soon as any CTA has given
 // up (the abort word), the CTA records ST_SOLVE_TIMEOUT and finishes
 // without waiting; the host then reports the step as failed.
@@ -202,12 +207,15 @@ __device__ __forceinline__ bool wait_panel(const unsigned* flags, int a, unsigne
     return ok;
 }
 
-__device__ __forceinline__ void load_linv(const cd* __restrict__ linv, int j0, int b, double2* Ls)
+// Rows [j0, j0 + b) of a per-panel 64-column block (linv, lmf, lnb) into
+// Ls[r][q] for q < bq, zeros elsewhere.
+__device__ __forceinline__ void load_linv(const cd* __restrict__ linv, int j0, int b, double2* Ls, int bq = -1)
 {
+    if (bq < 0) bq = b;
     for (int e = threadIdx.x; e < LDL_NB * LDL_NB; e += blockDim.x) {
         const int r = e / LDL_NB, q = e % LDL_NB;
         double2 v = make_double2(0.0, 0.0);
-        if (r < b && q < b) {
+        if (r < b && q < bq) {
             const cd a = ld2(linv + (size_t)(j0 + r) * LDL_NB + q);
             v = make_double2(a.x, a.y);
         }
@@ -216,20 +224,24 @@ __device__ __forceinline__ void load_linv(const cd* __restrict__ linv, int j0, i
 }
 
 // Forward: y_j = Linv_j (w_j - sum_{a<j} U(a, j)^H y_a), z_j = invD_j y_j.
+template <bool NEIGH>
 __global__ void __launch_bounds__(256) k_fwd_coop(const cd* __restrict__ A, int ld, const int* __restrict__ bstart,
                                                   int nb, const cd* __restrict__ w, cd* __restrict__ y,
                                                   cd* __restrict__ z, const cd* __restrict__ invD,
-                                                  const cd* __restrict__ linv, unsigned* __restrict__ flags,
-                                                  unsigned epoch, int* __restrict__ status, int* abort_word)
+                                                  const cd* __restrict__ linv, const cd* __restrict__ lmf,
+                                                  unsigned* __restrict__ flags, unsigned epoch,
+                                                  int* __restrict__ status, int* abort_word)
 {
     extern __shared__ double2 sm[];
     double2* Ls = sm;                          // Linv_j, [r][q]
     double2* red = sm + LDL_NB * LS_LD;        // [8][64] warp partials, then [4][64]
+    double2* Ms = red + 8 * LDL_NB;            // NEIGH: M_j, [r][q]
     __shared__ double2 t[LDL_NB];
     const int j = blockIdx.x;
     const int j0 = bstart[j], j1 = bstart[j + 1], b = j1 - j0;
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     load_linv(linv, j0, b, Ls);
+    if (NEIGH && j > 0) load_linv(lmf, j0, b, Ms, j0 - bstart[j - 1]);
     // this panel's right-hand side and pivots, read before the waits
     const cd wj = (threadIdx.x < b) ? ld2(w + j0 + threadIdx.x) : mk(0.0, 0.0);
     const cd dj = (threadIdx.x < b) ? ld2(invD + j0 + threadIdx.x) : mk(0.0, 0.0);
@@ -238,7 +250,10 @@ __global__ void __launch_bounds__(256) k_fwd_coop(const cd* __restrict__ A, int 
 #pragma unroll
     for (int m = 0; m < 8; m++) acc[m] = mk(0.0, 0.0);
     bool ok = true;
-    for (int a = 0; a < j; a++) {
+    // every panel but the previous one; that one comes in below through
+    // M_j = Linv_j U(j-1, j)^H
+    const int alast = NEIGH ? j - 1 : j;
+    for (int a = 0; a < alast; a++) {
         const int a0 = bstart[a], a1 = bstart[a + 1];
         const int r0 = a0 + lane, r1 = a0 + lane + 32;
         // the factor block U(panel a, panel j) does not depend on panel a's
@@ -287,13 +302,39 @@ __global__ void __launch_bounds__(256) k_fwd_coop(const cd* __restrict__ A, int 
         red[g * LDL_NB + r] = make_double2(s.x, s.y);
     }
     __syncthreads();
+    cd ys = mk(0.0, 0.0);
     if (threadIdx.x < b) {
         const int r = threadIdx.x;
-        cd s = mk(0.0, 0.0);
 #pragma unroll
-        for (int g = 0; g < 4; g++) s = s + mk(red[g * LDL_NB + r].x, red[g * LDL_NB + r].y);
-        y[j0 + r] = s;
-        z[j0 + r] = cmul(s, dj);
+        for (int g = 0; g < 4; g++) ys = ys + mk(red[g * LDL_NB + r].x, red[g * LDL_NB + r].y);
+    }
+    if (NEIGH && j > 0) {
+        // y_j -= M_j y_{j-1}: row r = tid & 63, columns g, g + 4, ...
+        const int a0 = bstart[j - 1], bp = j0 - a0;
+        const int r = threadIdx.x & 63, g = threadIdx.x >> 6;
+        // (the barrier inside also orders the reads of red above before the writes below)
+        if (wait_panel(flags, j - 1, epoch, status, abort_word, ok)) {
+            cd s = mk(0.0, 0.0);
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                const int q = g + 4 * i;
+                if (q < bp) {
+                    const double2 m = Ms[r * LS_LD + q];
+                    s = cfma(mk(m.x, m.y), ldcg2(y + a0 + q), s);
+                }
+            }
+            red[g * LDL_NB + r] = make_double2(s.x, s.y);
+        }
+        __syncthreads();
+        if (ok && threadIdx.x < b) {
+            const int rr = threadIdx.x;
+#pragma unroll
+            for (int g2 = 0; g2 < 4; g2++) ys = ys - mk(red[g2 * LDL_NB + rr].x, red[g2 * LDL_NB + rr].y);
+        }
+    }
+    if (threadIdx.x < b) {
+        y[j0 + threadIdx.x] = ys;
+        z[j0 + threadIdx.x] = cmul(ys, dj);
     }
     // the release by thread 0 after the barrier publishes every thread's
     // stores above (cumulativity of the gpu-scope release)
@@ -302,23 +343,30 @@ __global__ void __launch_bounds__(256) k_fwd_coop(const cd* __restrict__ A, int 
 }
 
 // Backward: x_j = Linv_j^H (z_j - sum_{c>j} U(j, c) x_c).
+template <bool NEIGH>
 __global__ void __launch_bounds__(256) k_bwd_coop(const cd* __restrict__ A, int ld, const int* __restrict__ bstart,
                                                   int nb, const cd* __restrict__ z, cd* __restrict__ x,
-                                                  const cd* __restrict__ linv, unsigned* __restrict__ flags,
-                                                  unsigned epoch, int* __restrict__ status, int* abort_word)
+                                                  const cd* __restrict__ linv, const cd* __restrict__ lnb,
+                                                  unsigned* __restrict__ flags, unsigned epoch,
+                                                  int* __restrict__ status, int* abort_word)
 {
     extern __shared__ double2 sm[];
     double2* Ls = sm;
     double2* red = sm + LDL_NB * LS_LD;  // [8][64]
+    double2* Ns = red + 8 * LDL_NB;      // NEIGH: N_j, [r][q]
     __shared__ double2 t[LDL_NB];
     const int j = blockIdx.x;
     const int j0 = bstart[j], j1 = bstart[j + 1], b = j1 - j0;
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     load_linv(linv, j0, b, Ls);
+    if (NEIGH && j + 1 < nb) load_linv(lnb, j0, b, Ns, bstart[j + 2] - j1);
     const cd zj = (threadIdx.x < b) ? ld2(z + j0 + threadIdx.x) : mk(0.0, 0.0);  // read before the waits
     cd a0 = mk(0.0, 0.0), a1 = mk(0.0, 0.0);  // rows lane, lane + 32
     bool ok = true;
-    for (int c = nb - 1; c > j; c--) {
+    // every later panel but the next one; that one comes in below through
+    // N_j = Linv_j^H U(j, j+1)
+    const int clast = NEIGH ? j + 1 : j;
+    for (int c = nb - 1; c > clast; c--) {
         const int c0 = bstart[c], c1 = bstart[c + 1];
         // U(panel j, panel c) before the wait for panel c's solution
         cd u0[8], u1[8];
@@ -361,13 +409,36 @@ __global__ void __launch_bounds__(256) k_bwd_coop(const cd* __restrict__ A, int 
         red[g * LDL_NB + r] = make_double2(s.x, s.y);
     }
     __syncthreads();
+    cd xs = mk(0.0, 0.0);
     if (threadIdx.x < b) {
         const int r = threadIdx.x;
-        cd s = mk(0.0, 0.0);
 #pragma unroll
-        for (int g = 0; g < 4; g++) s = s + mk(red[g * LDL_NB + r].x, red[g * LDL_NB + r].y);
-        x[j0 + r] = s;
+        for (int g = 0; g < 4; g++) xs = xs + mk(red[g * LDL_NB + r].x, red[g * LDL_NB + r].y);
     }
+    if (NEIGH && j + 1 < nb) {
+        // x_j -= N_j x_{j+1}: row r = tid & 63, columns g, g + 4, ...
+        const int c0 = bstart[j + 1], bn = bstart[j + 2] - c0;
+        const int r = threadIdx.x & 63, g = threadIdx.x >> 6;
+        if (wait_panel(flags, j + 1, epoch, status, abort_word, ok)) {
+            cd s = mk(0.0, 0.0);
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                const int q = g + 4 * i;
+                if (q < bn) {
+                    const double2 m = Ns[r * LS_LD + q];
+                    s = cfma(mk(m.x, m.y), ldcg2(x + c0 + q), s);
+                }
+            }
+            red[g * LDL_NB + r] = make_double2(s.x, s.y);
+        }
+        __syncthreads();
+        if (ok && threadIdx.x < b) {
+            const int rr = threadIdx.x;
+#pragma unroll
+            for (int g2 = 0; g2 < 4; g2++) xs = xs - mk(red[g2 * LDL_NB + rr].x, red[g2 * LDL_NB + rr].y);
+        }
+    }
+    if (threadIdx.x < b) x[j0 + threadIdx.x] = xs;
     __syncthreads();
     if (threadIdx.x == 0) st_release(flags + j, epoch);
 }
@@ -495,23 +566,37 @@ __global__ void k_vec_scale(cd* __restrict__ v, int n, double s)
 }
 
 // ---------------------------------------------------------------------------
-static size_t coop_smem() { return (size_t)(LDL_NB * LS_LD + 8 * LDL_NB) * sizeof(double2); }
-
-// Largest grid the cooperative solves may use on this device (0: none).
-static int coop_capacity(Ctx& c)
+// Shared memory of the cooperative solves: the inverse diagonal block, the
+// partial sums and, with NEIGH, the neighbour product M_j / N_j.
+static size_t coop_smem(bool neigh)
 {
-    if (c.coop_max_blocks) return c.coop_max_blocks;
-    const int sm = (int)coop_smem();
-    cudaFuncSetAttribute(k_fwd_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    cudaFuncSetAttribute(k_bwd_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    return (size_t)(LDL_NB * LS_LD + 8 * LDL_NB + (neigh ? LDL_NB * LS_LD : 0)) * sizeof(double2);
+}
+
+template <bool NEIGH>
+static int coop_blocks(int dev)
+{
+    const int sm = (int)coop_smem(NEIGH);
+    cudaFuncSetAttribute(k_fwd_coop<NEIGH>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(k_bwd_coop<NEIGH>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     int coop = 0, nsm = 0, per1 = 0, per2 = 0;
-    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c.dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, k_fwd_coop, 256, sm);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_bwd_coop, 256, sm);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, k_fwd_coop<NEIGH>, 256, sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_bwd_coop<NEIGH>, 256, sm);
     cudaGetLastError();
-    c.coop_max_blocks = coop ? nsm * std::min(per1, per2) : -1;
-    return c.coop_max_blocks;
+    return coop ? nsm * std::min(per1, per2) : -1;
+}
+
+// Largest grid the cooperative solves may use on this device (-1: none),
+// without and with the neighbour products.
+static int coop_capacity(Ctx& c, bool neigh)
+{
+    if (!c.coop_max_blocks) {
+        c.coop_max_blocks = coop_blocks<false>(c.dev);
+        c.coop_max_neigh = coop_blocks<true>(c.dev);
+    }
+    return neigh ? c.coop_max_neigh : c.coop_max_blocks;
 }
 
 static int solve_multi_launch(Ctx& c, int n)
@@ -539,10 +624,10 @@ static int solve_multi_launch(Ctx& c, int n)
     return 0;
 }
 
-static int solve_cooperative(Ctx& c, int n)
+static int solve_cooperative(Ctx& c, int n, bool neigh)
 {
     int nb = (int)c.blk_start.size();
-    const size_t sm = coop_smem();
+    const size_t sm = coop_smem(neigh);
     int* abort_word = c.counters + 2;
     if (cudaMemsetAsync(abort_word, 0, sizeof(int), c.stream) != cudaSuccess) return -2;
     const int* bs = c.dblk;
@@ -550,16 +635,20 @@ static int solve_cooperative(Ctx& c, int n)
     const cd* w = c.w;
     const cd* invD = c.invD;
     const cd* linv = c.linv;
+    const cd* lmf = c.lmf;
+    const cd* lnb = c.lnb;
     int ld = c.ld;
+    const void* kf = neigh ? (const void*)k_fwd_coop<true> : (const void*)k_fwd_coop<false>;
+    const void* kb = neigh ? (const void*)k_bwd_coop<true> : (const void*)k_bwd_coop<false>;
     unsigned e1 = ++c.epoch;
-    void* a1[] = {(void*)&H, &ld, (void*)&bs, &nb, (void*)&w, &c.yv, &c.zv, (void*)&invD, (void*)&linv, &c.flags,
-                  &e1, &c.status, &abort_word};
-    if (cudaLaunchCooperativeKernel((const void*)k_fwd_coop, nb, 256, a1, sm, c.stream) != cudaSuccess) return -2;
+    void* a1[] = {(void*)&H, &ld, (void*)&bs, &nb, (void*)&w, &c.yv, &c.zv, (void*)&invD, (void*)&linv, (void*)&lmf,
+                  &c.flags, &e1, &c.status, &abort_word};
+    if (cudaLaunchCooperativeKernel(kf, nb, 256, a1, sm, c.stream) != cudaSuccess) return -2;
     unsigned e2 = ++c.epoch;
     const cd* zv = c.zv;
-    void* a2[] = {(void*)&H, &ld, (void*)&bs, &nb, (void*)&zv, &c.x, (void*)&linv, &c.flags, &e2, &c.status,
-                  &abort_word};
-    if (cudaLaunchCooperativeKernel((const void*)k_bwd_coop, nb, 256, a2, sm, c.stream) != cudaSuccess) return -2;
+    void* a2[] = {(void*)&H, &ld, (void*)&bs, &nb, (void*)&zv, &c.x, (void*)&linv, (void*)&lnb, &c.flags, &e2,
+                  &c.status, &abort_word};
+    if (cudaLaunchCooperativeKernel(kb, nb, 256, a2, sm, c.stream) != cudaSuccess) return -2;
     c.launches += 2;
     return 0;
 }
@@ -569,7 +658,15 @@ int invit_step(Ctx& c, int n, bool /*first*/)
     k_hemv<<<(n * 32 + 255) / 256, 256, 0, c.stream>>>(c.S, c.ld, n, c.c, c.w);
     c.launches++;
     const int nb = (int)c.blk_start.size();
-    int r = (nb <= coop_capacity(c)) ? solve_cooperative(c, n) : solve_multi_launch(c, n);
+    // the neighbour products take a second 64 x 64 block of shared memory
+    // (one CTA per SM): used while every panel still has an SM of its own
+    int r;
+    if (nb <= coop_capacity(c, true))
+        r = solve_cooperative(c, n, true);
+    else if (nb <= coop_capacity(c, false))
+        r = solve_cooperative(c, n, false);
+    else
+        r = solve_multi_launch(c, n);
     if (r) return r;
     k_iter_norm<<<1, 1024, 0, c.stream>>>(n, c.x, c.c, sqrt(2.0 * n), c.red);
     c.launches++;

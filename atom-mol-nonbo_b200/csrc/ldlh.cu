@@ -14,7 +14,9 @@
 //   k_ldl_trsm    Wun(p, c) by substitution with U_pp, U(p, c) = invD Wun;
 //   k_ldl_bulk    W(r, c) -= sum_q conj(U(q,r)) Wun(q,c), r <= c beyond p
 //                 (the Hermitian trailing update, a complex GEMM);
-//   k_ldl_linv    after the last panel: (U_pp^H)^-1 of every new panel.
+//   k_ldl_linv    after the last panel: (U_pp^H)^-1 of every new panel;
+//   k_ldl_mn      then the neighbour products Linv_p U(p-1, p)^H and
+//                 Linv_p^H U(p, p+1) the cooperative solves apply.
 // The off-diagonal recurrence and the pivot d = conj(.) follow
 // src/linalg.f90:359-391 term for term; only the summation order differs,
 // and the pivots are kept real (the reference's complex arithmetic leaves a
@@ -315,6 +317,74 @@ __global__ void __launch_bounds__(256) k_ldl_linv(const cd* __restrict__ A, int 
         const int r = e >> 6, s2 = e & 63;
         const double2 v = X[r * DG_LD + s2];
         linv[(size_t)(p0 + r) * LDL_NB + s2] = cd{v.x, v.y};
+    }
+}
+
+// Neighbour products of the cooperative triangular solves (invit.cu), for
+// the panels j in [first, nb): M_j = Linv_j U(j-1, j)^H (blockIdx.y = 0,
+// j >= 1) and N_j = Linv_j^H U(j, j+1) (blockIdx.y = 1, j + 1 < nb), each
+// stored like linv, row r of panel j at [(p0 + r) * 64 + q].  With them a
+// solve's panel j applies the neighbouring panel's solution as one 64 x 64
+// product once that panel is published, everything else being done before.
+__global__ void __launch_bounds__(256) k_ldl_mn(const cd* __restrict__ A, int ld, const int* __restrict__ bstart,
+                                                 int nb, int first, const cd* __restrict__ linv, cd* __restrict__ lmf,
+                                                 cd* __restrict__ lnb)
+{
+    extern __shared__ double2 sm[];
+    double2* Ls = sm;                   // Ls[r * DG_LD + c] = Linv_j(r, c)
+    double2* Us = sm + LDL_NB * DG_LD;  // Us[c * DG_LD + q]: conj(U(o0 + q, p0 + c)) or U(p0 + c, o0 + q)
+    const int j = first + blockIdx.x;
+    const bool fwd = blockIdx.y == 0;
+    if (fwd ? j < 1 : j + 1 >= nb) return;
+    const int p0 = bstart[j], b = bstart[j + 1] - p0;
+    const int o0 = fwd ? bstart[j - 1] : bstart[j + 1];
+    const int bo = fwd ? p0 - o0 : bstart[j + 2] - o0;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < LDL_NB * LDL_NB; e += 256) {
+        const int c = e & 63, r = e >> 6;
+        double2 v = make_double2(0.0, 0.0);
+        if (r < b && c < b) {
+            const cd x = linv[(size_t)(p0 + r) * LDL_NB + c];
+            v = make_double2(x.x, x.y);
+        }
+        Ls[r * DG_LD + c] = v;
+        // the neighbour block, read along its columns
+        const int lo = e & 63, hi = e >> 6;
+        double2 u = make_double2(0.0, 0.0);
+        if (fwd) {
+            if (hi < b && lo < bo) {
+                const cd x = A[(size_t)(o0 + lo) + (size_t)(p0 + hi) * ld];
+                u = make_double2(x.x, -x.y);
+            }
+            Us[hi * DG_LD + lo] = u;
+        } else {
+            if (lo < b && hi < bo) {
+                const cd x = A[(size_t)(p0 + lo) + (size_t)(o0 + hi) * ld];
+                u = make_double2(x.x, x.y);
+            }
+            Us[lo * DG_LD + hi] = u;
+        }
+    }
+    __syncthreads();
+    const int r = tid >> 2, q0 = tid & 3;
+    double accr[16], acci[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) accr[i] = acci[i] = 0.0;
+    const int c0 = fwd ? 0 : r, c1 = fwd ? r + 1 : LDL_NB;
+    for (int c = c0; c < c1; c++) {
+        double2 l = fwd ? Ls[r * DG_LD + c] : Ls[c * DG_LD + r];
+        if (!fwd) l.y = -l.y;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const double2 u = Us[c * DG_LD + q0 + 4 * i];
+            accr[i] = fma(l.x, u.x, fma(-l.y, u.y, accr[i]));
+            acci[i] = fma(l.x, u.y, fma(l.y, u.x, acci[i]));
+        }
+    }
+    if (r < b) {
+        cd* out = (fwd ? lmf : lnb) + (size_t)(p0 + r) * LDL_NB;
+#pragma unroll
+        for (int i = 0; i < 16; i++) out[q0 + 4 * i] = cd{accr[i], acci[i]};
     }
 }
 
@@ -623,7 +693,10 @@ static void enqueue_factor(Ctx& c, int m0, int n, const std::vector<int>& starts
     }
     if (nblk > nexist) {
         k_ldl_linv<<<nblk - nexist, 256, 2 * sm1, c.stream>>>(c.F, c.ld, c.dblk, nexist, c.linv);
-        c.launches++;
+        // the last existing panel's N changes with the first new panel
+        const int f = std::max(nexist - 1, 0);
+        k_ldl_mn<<<dim3(nblk - f, 2), 256, 2 * sm1, c.stream>>>(c.F, c.ld, c.dblk, nblk, f, c.linv, c.lmf, c.lnb);
+        c.launches += 2;
     }
 }
 
@@ -638,7 +711,9 @@ static void enqueue_persist(Ctx& c, int n, const unsigned* tasks, int ntasks, un
     ldlp_enqueue(c, n, tasks, ntasks, trace);
     const int nblk = (n + LDL_NB - 1) / LDL_NB;
     k_ldl_linv<<<nblk, 256, 2 * LDL_NB * DG_LD * sizeof(double2), c.stream>>>(c.F, c.ld, c.dblk, 0, c.linv);
-    c.launches++;
+    k_ldl_mn<<<dim3(nblk, 2), 256, 2 * LDL_NB * DG_LD * sizeof(double2), c.stream>>>(c.F, c.ld, c.dblk, nblk, 0,
+                                                                                    c.linv, c.lmf, c.lnb);
+    c.launches += 2;
 }
 
 static void ldl_attrs()
@@ -649,6 +724,7 @@ static void ldl_attrs()
     cudaFuncSetAttribute(k_ldl_diag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DG_SMEM);
     cudaFuncSetAttribute(k_ldl_diag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DG_SMEM);
     cudaFuncSetAttribute(k_ldl_linv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * sm1));
+    cudaFuncSetAttribute(k_ldl_mn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * sm1));
     cudaFuncSetAttribute(k_ldl_bulk<32, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem<32>());
     cudaFuncSetAttribute(k_ldl_bulk<16, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem<16>());
     g_ldl_attr = true;
