@@ -96,10 +96,11 @@ CONFIGS = {
 }
 
 
-# configs[4] names "5 particles: one heavy particle and three electrons,
-# n = 4": the particle list describes the n = 3 Li-like system of
-# CONFIGS[4]; the five-particle n = 4 reading is this one (heavy particle
-# and four electrons), with the same seed, size and mass scaling.
+# The K = 10000 workload is described as "5 particles: one heavy particle
+# and three electrons, n = 4": that particle list is the n = 3 Li-like
+# system of entry 4 above; the five-particle n = 4 reading is this one
+# (heavy particle and four electrons), with the same seed, size and mass
+# scaling.
 CONFIG4_N4 = dict(system="li_minus_like", K=10000, seed=1004, mass_scaled=True)
 
 

@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--cpu-baseline", type=int, default=1)
     ap.add_argument("--candidates", type=int, default=1, help="also time the batched-candidate configuration")
-    ap.add_argument("--large", type=int, default=1, help="also run configs[4]'s K=10000 step (n=3 and n=4)")
+    ap.add_argument("--large", type=int, default=1, help="also run the K=10000 step (Li-like n=3 and five-particle n=4)")
     ap.add_argument("--large-K", type=int, default=10000)
     ap.add_argument("--composite", type=int, default=1,
                     help="also time one new function's energy + gradient at K: plain, adjoint, batched")
@@ -415,9 +415,9 @@ def run_ours(args, dist):
         comp = run_composite(args, dev, dist.rank, lam)
         comp["full_gradient"] = {"adjoint_ms": ms_step, "plain_ms": plain["ms_per_step"] if plain else None,
                                  "speedup": (plain["ms_per_step"] / ms_step) if plain else None}
-        line["north_star"] = comp
+        line["composite"] = comp
     if args.large:
-        line["configs4_k10000"] = run_large(args, dev, dist.rank)
+        line["large_k10000"] = run_large(args, dev, dist.rank)
     if args.candidates:
         line["candidates"] = run_candidates(args, dev, dist.rank, cpu=bool(args.cpu_baseline and dist.rank == 0))
     if args.expc:
@@ -537,7 +537,7 @@ def run_composite(args, dev, rank, lam):
 
 
 def run_large(args, dev, rank):
-    """configs[4], K = 10000: one full energy + gradient step (H, S build,
+    """The largest workload, K = 10000: one full energy + gradient step (H, S build,
     LDL^H, inverse iteration at Tol 1e-12, fused adjoint gradient) for the
     Li-like n = 3 system (six Y^+Y terms) and for the five-particle n = 4
     system (heavy particle + four electrons, 14 terms), mass-scaled seeded

@@ -1,5 +1,5 @@
 """n = 4 (five particles: heavy particle + four electrons, 14 Y^+Y terms,
-the n = 4 reading of configs[4]) through the whole path on the GPU against
+the n = 4 reading of the K = 10000 five-particle workload) through the whole path on the GPU against
 the oracle: every stored element of H and S (ComputeMatElem + StoreHS,
 src/matform.f90:11-51,119-230), the energy of GHEPIIS (src/linalg.f90:
 1781-1926), and the EnergyIB gradient (src/workproc.f90:2063-2154) in the
