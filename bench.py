@@ -370,7 +370,7 @@ def run_ours(args, dist):
         "ldlh": roof("tensor", ldl_flop, st[1], peak_tc, "TFLOP/s",
                      "LDL^H factorisation, one CUDA-graph launch per step: the persistent tile kernel "
                      "k_ldl_persist (trailing updates and panel rows on the FP64 tensor cores, the diagonal "
-                     "chain on its own CTA) between k_ldl_mirror and k_ldl_linv", tc_src, "ldlh"),
+                     "chain on its own CTA) between k_ldl_mirror and k_ldl_linv + k_ldl_mn", tc_src, "ldlh"),
         "invit": roof("hbm", invit_bytes, st[2], peaks["hbm_gbs"], "GB/s",
                       "inverse iterations (k_hemv, k_fwd_coop, k_bwd_coop) + Rayleigh quotient", hbm_src, "invit"),
         "adjoint": roof("fp64", adj_flop, st[3], peak_fma, "TFLOP/s",
